@@ -1,0 +1,125 @@
+/* praq.h -- C ABI of the B200 PRAQ solver (QUBO roof-dual LP by restarted,
+ * reflected Halpern PDHG on the half-edge lift).
+ *
+ * The first block is a drop-in for the reference's libpraq.so: the same entry
+ * points, struct layouts, argument meaning and error codes, so the reference's
+ * ctypes `Library` (qubo/harness/praq_cuda_library.py:90-139) and its file CLI
+ * contract bind to this library unchanged.
+ *
+ *   PraqInstance / PraqParameters / PraqResult  replace
+ *       qubo/praq-cuda/include/praq/praq.h:20-67 (field for field)
+ *   praq_default_parameters   replaces qubo/praq-cuda/include/praq/praq.h:71
+ *                             (defaults of Parameters.with_auto_step,
+ *                             qubo/praq-jax/praq/solver.py:129-164)
+ *   praq_check_interval       replaces qubo/praq-cuda/include/praq/praq.h:76
+ *   praq_solve                replaces qubo/praq-cuda/include/praq/praq.h:85-86
+ *
+ * The second block (reform_praq_*) has no counterpart in the reference: it
+ * splits a solve into set-up (validation, device layout, upload) and repeated
+ * device-resident solves on a caller-supplied CUDA stream, which is what the
+ * batch engine and the timing harness need.
+ *
+ * All host pointers are caller-owned and only read (outputs only written).
+ * Every call is thread-safe: each solve runs on its own stream and device
+ * allocations, and touches neither the legacy default stream nor other
+ * solves' memory.
+ */
+#ifndef REFORM_B200_PRAQ_H
+#define REFORM_B200_PRAQ_H
+
+#include <stdint.h>
+
+#ifndef REFORM_API
+#define REFORM_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* min_{x in {0,1}^n} x^T W x; W symmetric, diagonal + strict upper COO. */
+typedef struct {
+    int64_t n;              /* binary variables                                 */
+    int64_t m;              /* off-diagonal nonzeros (edges), rows[e] != cols[e] */
+    const double* diag;     /* [n]                                              */
+    const int64_t* rows;    /* [m]                                              */
+    const int64_t* cols;    /* [m]                                              */
+    const double* vals;     /* [m], W_ij = W_ji                                 */
+} PraqInstance;
+
+typedef struct {
+    double tolerance;       /* relative duality gap at termination              */
+    int64_t max_iter;       /* <= 0: no cap                                     */
+    int use_float32;        /* 0: FP64 iterates; 1: FP32 iterates with FP64
+                               reductions, restart logic and bounds            */
+    double omega;           /* initial primal weight                            */
+    double beta_sufficient;
+    double beta_necessary;
+    double beta_artificial;
+    double theta_initial;
+    double theta_target;
+    double theta_decay;
+    int64_t op_steps;       /* iterations between checks (>= 2); <= 0: the rule */
+    double interval_offset; /* check-interval rule, see praq_check_interval    */
+    double interval_scale;
+    double interval_power;
+} PraqParameters;
+
+typedef struct {
+    double lower;           /* valid lower bound on the relaxation optimum      */
+    double upper;           /* relaxation value F(x) at the returned primal     */
+    int64_t iterations;
+    int status;             /* 0 converged, 1 iteration limit, < 0 error        */
+} PraqResult;
+
+/* Error codes (negative), as the reference's. */
+#define PRAQ_ERROR_ARGUMENT (-1)   /* null pointer or bad parameter             */
+#define PRAQ_ERROR_INSTANCE (-2)   /* index out of range, self-loop, n = 0,
+                                      or sizes beyond int32 indexing            */
+#define PRAQ_ERROR_CUDA     (-3)   /* any CUDA runtime failure                  */
+
+REFORM_API PraqParameters praq_default_parameters(void);
+
+/* max(2, round(offset + scale * B(ln(n / 50000), power))), B the Box-Cox
+ * transform; 2 for a null pointer or n <= 0. */
+REFORM_API int64_t praq_check_interval(int64_t n, const PraqParameters* parameters);
+
+/* Solve the roof-dual LP.  x receives the primal [n].  Returns result->status. */
+REFORM_API int praq_solve(const PraqInstance* instance, const PraqParameters* parameters,
+               double* x, PraqResult* result);
+
+/* ---- device-resident solves (no reference counterpart) ------------------- */
+
+typedef struct reform_praq_solver reform_praq_solver;
+
+/* Validate, lay the instance out on the device and capture the iteration
+ * graphs, on `stream` (a cudaStream_t; NULL makes a private non-blocking
+ * stream).  Returns 0 or a PRAQ_ERROR_* code. */
+REFORM_API int reform_praq_create(const PraqInstance* instance, const PraqParameters* parameters,
+                       void* stream, reform_praq_solver** out);
+
+/* One full solve from the cold start on the device-resident instance.  Blocks
+ * the host until the solve has finished (the restart/termination decisions are
+ * taken on the device; the host only watches a flag).  Returns the status. */
+REFORM_API int reform_praq_run(reform_praq_solver* solver);
+
+/* The last run's primal (x may be NULL), dual pairs in instance units
+ * (y2 [2m], may be NULL) and result. */
+REFORM_API int reform_praq_result(reform_praq_solver* solver, double* x, double* y2, PraqResult* result);
+
+/* A wall-clock budget for each run, in seconds (< 0: none, the default).
+ * When it runs out the run stops between two checks and returns
+ * PRAQ_STATUS_TIME_LIMIT; the result is the bracket of the last completed
+ * check (valid: both iterates stay feasible) and the current primal iterate. */
+#define PRAQ_STATUS_TIME_LIMIT 2
+REFORM_API int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds);
+
+/* Kernel launches the last run issued (graph kernel nodes included). */
+REFORM_API int64_t reform_praq_launches(const reform_praq_solver* solver);
+
+REFORM_API void reform_praq_destroy(reform_praq_solver* solver);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REFORM_B200_PRAQ_H */

@@ -1,0 +1,100 @@
+"""ctypes binding of libreform_b200.so, the C ABI declared in include/*.h.
+
+There is no fallback: if the library is missing or fails to load, every solve
+raises.  The structs mirror the headers field for field (the PRAQ and PRIA ones
+are byte-compatible with the reference's praq.h / pria.h).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_int, c_int64, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libreform_b200.so"
+
+
+class PraqInstance(ctypes.Structure):
+    _fields_ = [("n", c_int64), ("m", c_int64), ("diag", POINTER(c_double)),
+                ("rows", POINTER(c_int64)), ("cols", POINTER(c_int64)),
+                ("vals", POINTER(c_double))]
+
+
+class PraqParameters(ctypes.Structure):
+    _fields_ = [("tolerance", c_double), ("max_iter", c_int64), ("use_float32", c_int),
+                ("omega", c_double), ("beta_sufficient", c_double),
+                ("beta_necessary", c_double), ("beta_artificial", c_double),
+                ("theta_initial", c_double), ("theta_target", c_double),
+                ("theta_decay", c_double), ("op_steps", c_int64),
+                ("interval_offset", c_double), ("interval_scale", c_double),
+                ("interval_power", c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PraqResult(ctypes.Structure):
+    _fields_ = [("lower", c_double), ("upper", c_double), ("iterations", c_int64),
+                ("status", c_int)]
+
+
+class PriaParams(ctypes.Structure):
+    _fields_ = [("omega", c_double), ("eta", c_double), ("beta_sufficient", c_double),
+                ("beta_artificial", c_double), ("beta_necessary", c_double),
+                ("theta_initial", c_double), ("theta_target", c_double),
+                ("theta_decay", c_double), ("tolerance", c_double), ("max_iter", c_int64),
+                ("use_halpern", c_int), ("warm_steps", c_int), ("op_steps", c_int),
+                ("verbose", c_int)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PriaResultInfo(ctypes.Structure):
+    _fields_ = [("iterations", c_int64), ("primal_objective", c_double),
+                ("dual_objective", c_double), ("relative_gap", c_double)]
+
+
+_lib = None
+
+
+def _declare(lib):
+    D, I, L = POINTER(c_double), c_int, c_int64
+    P = ctypes.POINTER
+    sig = {
+        "praq_default_parameters": (PraqParameters, []),
+        "praq_check_interval": (c_int64, [c_int64, P(PraqParameters)]),
+        "praq_solve": (I, [P(PraqInstance), P(PraqParameters), D, P(PraqResult)]),
+        "reform_praq_create": (I, [P(PraqInstance), P(PraqParameters), c_void_p,
+                                   P(c_void_p)]),
+        "reform_praq_run": (I, [c_void_p]),
+        "reform_praq_result": (I, [c_void_p, D, D, P(PraqResult)]),
+        "reform_praq_set_time_limit": (I, [c_void_p, c_double]),
+        "reform_praq_launches": (c_int64, [c_void_p]),
+        "reform_praq_destroy": (None, [c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def lib():
+    """The loaded native library; raises if it is absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is not built; run `python -m reformulation_b200.build`. "
+                "There is no CPU fallback.")
+        _lib = _declare(ctypes.CDLL(str(LIB_PATH)))
+    return _lib
+
+
+def dptr(a):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def iptr(a):
+    return a.ctypes.data_as(POINTER(c_int64))

@@ -1,0 +1,107 @@
+// common.cuh -- shared device/host helpers for the PRAQ and PRIA solvers.
+//
+// Everything here is plain sm_100a CUDA C++: warp shuffles, shared memory and
+// fixed-order block reductions (deterministic: the order of additions depends
+// on the launch shape only, so a solve is bitwise reproducible run to run).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <limits>
+#include <vector>
+
+namespace rb200 {
+
+constexpr int kWarp = 32;
+
+#define RB_CUDA_TRY(call)                                      \
+    do {                                                       \
+        cudaError_t rb_err_ = (call);                          \
+        if (rb_err_ != cudaSuccess) return rb_err_;            \
+    } while (0)
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum K doubles over the block; the total lands in out[0..K) (written by
+// thread 0).  Fixed order: butterfly within each warp, then warp 0 adds the
+// per-warp totals in warp order.  `scratch` holds K * 32 doubles.
+template <int K>
+__device__ __forceinline__ void block_sums(double (&v)[K], double* scratch, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = warp_sum(v[k]);
+        if (lane == 0) scratch[k * 32 + warp] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < warps ? scratch[k * 32 + lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[k] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// Deterministic sum of `count` rows of K doubles (row-major, stride K) by one
+// block: thread t adds rows t, t + blockDim, ... in order, then block_sums.
+template <int K>
+__device__ __forceinline__ void reduce_rows(const double* rows, int count, double* scratch,
+                                            double* out) {
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    for (int r = threadIdx.x; r < count; r += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] += rows[size_t(r) * K + k];
+    }
+    block_sums<K>(v, scratch, out);
+}
+
+template <class T>
+__device__ __forceinline__ T clampv(T v, T lo, T hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// A device allocation on a stream (cudaMallocAsync), released on the same
+// stream.  The caller owns the stream and synchronises before it goes away.
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr) cudaFreeAsync(ptr, stream);
+        ptr = nullptr;
+        count = 0;
+    }
+    cudaError_t alloc(size_t n, cudaStream_t s) {
+        release();
+        stream = s;
+        count = n;
+        return cudaMallocAsync(reinterpret_cast<void**>(&ptr), sizeof(T) * (n ? n : 1), s);
+    }
+    cudaError_t upload(const T* host, size_t n, cudaStream_t s) {
+        RB_CUDA_TRY(alloc(n, s));
+        if (n) RB_CUDA_TRY(cudaMemcpyAsync(ptr, host, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+        return cudaSuccess;
+    }
+};
+
+inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+}  // namespace rb200

@@ -1,0 +1,197 @@
+"""PRAQ on B200: the Python face of the native solver.
+
+* `Library` mirrors the reference's in-process ctypes wrapper
+  (``qubo/harness/praq_cuda_library.py:90-139``): `parameters(**overrides)`,
+  `check_interval(n, parameters)`, `solve(instance, parameters) -> Solve`.
+* `DeviceSolver` keeps an instance resident on the GPU and solves it again and
+  again from the cold start (the timing harness and the serving engine use it).
+* `solve(instance, *, tolerances, time_limit, ...)` is the backend entry point,
+  the drop-in for ``qubo/harness/backends/praq_cuda.py:79-167``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from ctypes import c_void_p
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .results import QuboResult, Tolerances
+
+#: PraqParameters fields a caller may override (the reference's SCHEDULE,
+#: qubo/harness/praq_cuda_library.py:50-52).
+SCHEDULE = ("omega", "beta_sufficient", "beta_necessary", "beta_artificial",
+            "theta_initial", "theta_target", "theta_decay", "op_steps",
+            "interval_offset", "interval_scale", "interval_power")
+
+STATUS = {0: "optimal", 1: "iteration_limit", 2: "time_limit"}
+
+
+@dataclass(frozen=True)
+class Solve:
+    """What one solve returned (the reference's `Solve` record)."""
+
+    status: int
+    lower: float
+    upper: float
+    iterations: int
+    x: np.ndarray
+
+    @property
+    def gap(self) -> float:
+        return (self.upper - self.lower) / (1.0 + abs(self.upper) + abs(self.lower))
+
+
+class _View:
+    """Keeps the contiguous arrays alive while the C struct points at them."""
+
+    def __init__(self, instance):
+        self.diag = np.ascontiguousarray(instance.diag, dtype=np.float64)
+        self.rows = np.ascontiguousarray(instance.rows, dtype=np.int64)
+        self.cols = np.ascontiguousarray(instance.cols, dtype=np.int64)
+        self.vals = np.ascontiguousarray(instance.vals, dtype=np.float64)
+        self.struct = _native.PraqInstance(int(instance.n), int(self.vals.size),
+                                           _native.dptr(self.diag), _native.iptr(self.rows),
+                                           _native.iptr(self.cols), _native.dptr(self.vals))
+
+
+class Library:
+    """The native library, with the reference Library's three methods."""
+
+    def __init__(self):
+        self._lib = _native.lib()
+
+    def parameters(self, **overrides) -> _native.PraqParameters:
+        p = self._lib.praq_default_parameters()
+        names = dict(_native.PraqParameters._fields_)
+        for name, value in overrides.items():
+            if name not in names:
+                raise KeyError(f"PraqParameters has no field {name!r}")
+            setattr(p, name, value)
+        return p
+
+    def check_interval(self, n: int, parameters: _native.PraqParameters) -> int:
+        if parameters.op_steps > 0:
+            return max(int(parameters.op_steps), 2)
+        return int(self._lib.praq_check_interval(n, ctypes.byref(parameters)))
+
+    def solve(self, instance, parameters: _native.PraqParameters) -> Solve:
+        view = _View(instance)
+        x = np.empty(int(instance.n), dtype=np.float64)
+        result = _native.PraqResult()
+        status = self._lib.praq_solve(ctypes.byref(view.struct), ctypes.byref(parameters),
+                                      _native.dptr(x), ctypes.byref(result))
+        return Solve(int(status), result.lower, result.upper, int(result.iterations), x)
+
+
+class DeviceSolver:
+    """An instance laid out on the device once and solved any number of times.
+
+    `stream` is a raw cudaStream_t (e.g. ``torch.cuda.current_stream().cuda_stream``)
+    or None for a private stream."""
+
+    def __init__(self, instance, parameters: _native.PraqParameters | None = None,
+                 stream: int | None = None):
+        self._lib = _native.lib()
+        self.n, self.m = int(instance.n), int(np.asarray(instance.vals).size)
+        view = _View(instance)
+        self.parameters = parameters or self._lib.praq_default_parameters()
+        handle = c_void_p()
+        rc = self._lib.reform_praq_create(ctypes.byref(view.struct), ctypes.byref(self.parameters),
+                                          c_void_p(stream) if stream else None,
+                                          ctypes.byref(handle))
+        if rc != 0:
+            raise RuntimeError(f"reform_praq_create failed with status {rc}")
+        self._h = handle
+
+    def set_time_limit(self, seconds: float) -> None:
+        self._lib.reform_praq_set_time_limit(self._h, float(seconds))
+
+    def run(self) -> int:
+        return int(self._lib.reform_praq_run(self._h))
+
+    def result(self, want_x: bool = True, want_dual: bool = False):
+        x = np.empty(self.n) if want_x else None
+        y = np.empty(2 * max(self.m, 1)) if want_dual else None
+        r = _native.PraqResult()
+        rc = self._lib.reform_praq_result(self._h, _native.dptr(x) if x is not None else None,
+                                          _native.dptr(y) if y is not None else None,
+                                          ctypes.byref(r))
+        if rc != 0:
+            raise RuntimeError(f"reform_praq_result failed with status {rc}")
+        out = Solve(int(r.status), r.lower, r.upper, int(r.iterations), x)
+        if want_dual:
+            return out, y[:2 * self.m].reshape(-1, 2)
+        return out
+
+    def launches(self) -> int:
+        return int(self._lib.reform_praq_launches(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.reform_praq_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def solve(instance, *, tolerances: Tolerances = Tolerances(), time_limit: float = math.inf,
+          sample_memory: bool = False, precision: str = "fp64", max_iter: int | None = None,
+          **schedule) -> QuboResult:
+    """Solve the roof-dual relaxation of `instance` on the GPU.
+
+    The contract of the reference backend: only `tolerances.optimality` reaches
+    the solver, as the relative duality gap it stops on; `feasibility` stays
+    NaN in the record.  `time_limit` is a wall-clock budget checked between two
+    convergence checks (status "time_limit", with the bracket of the last
+    check).  `precision` is "fp64" or "mixed" (FP32 iterates, FP64 reductions
+    and bounds).  `schedule` overrides fields of `SCHEDULE`.  `sample_memory`
+    is accepted for signature compatibility; the device footprint is the
+    solver's own allocation and is not sampled.
+    """
+    common = dict(backend="praq-b200", instance=instance.name, family=instance.family,
+                  n=int(instance.n), edges=int(np.asarray(instance.vals).size),
+                  optimality_tolerance=tolerances.optimality)
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+    unknown = set(schedule) - set(SCHEDULE)
+    if unknown:
+        raise KeyError(f"not schedule fields: {sorted(unknown)}")
+    lib = Library()
+    p = lib.parameters(tolerance=tolerances.optimality, use_float32=int(precision == "mixed"),
+                       max_iter=-1 if max_iter is None else int(max_iter), **schedule)
+    start = time.perf_counter()
+    try:
+        solver = DeviceSolver(instance, p)
+    except RuntimeError as error:
+        return QuboResult(status="error", note=str(error)[:200], **common)
+    setup = time.perf_counter() - start
+    try:
+        if math.isfinite(time_limit):
+            solver.set_time_limit(max(0.0, time_limit - setup))
+        start = time.perf_counter()
+        code = solver.run()
+        res = solver.result(want_x=True)
+        seconds = time.perf_counter() - start
+    finally:
+        solver.close()
+    if code < 0:
+        return QuboResult(status="error", note=f"status {code}", setup_seconds=setup, **common)
+    status = STATUS.get(code, "error")
+    timed = dict(iterations=res.iterations, setup_seconds=setup, solve_seconds=seconds, **common)
+    if status != "optimal":
+        return QuboResult(status=status, lower=res.lower, upper=res.upper,
+                          note=f"status {code}, relative gap {res.gap:.3g}", **timed)
+    return QuboResult(status=status, objective=res.upper, lower=res.lower, upper=res.upper,
+                      note=f"precision {precision}", **timed)

@@ -1,0 +1,180 @@
+"""PRAQ on the GPU against the oracles, through the C ABI (praq_solve and the
+reform_praq_* device-resident API).
+
+Patterned on the reference's own checks (qubo/praq-cuda/tests/test_solver.cu:
+122-262 and qubo/praq-jax/tests/test_solver.py:40-135): the enumerated
+half-integral optimum on tiny instances, bounds that bracket the optimum under
+every iteration cap, FP32 reaching its own accuracy, a larger instance
+certifying its own gap, rejection of bad inputs; plus agreement with the CPU
+restatement (iterations and bounds) and with the max-flow roof dual.
+
+Tolerances: FP64 bounds agree with the optimum to 1e-7 relative at a 1e-9 gap;
+FP64 iteration counts agree with the oracle's exactly on these instances (same
+arithmetic, different summation order can move a check by one block, so
++-op_steps is allowed); FP32 ("mixed") results agree to 1e-3 relative at a 1e-4
+gap.
+"""
+
+import numpy as np
+import pytest
+
+from reformulation_b200.instances import QuboInstance, qubo_sparse_bernoulli
+
+pytestmark = pytest.mark.gpu
+
+
+def random_qubo(seed, n, density, magnitude=3):
+    rng = np.random.default_rng(seed)
+    iu = np.triu_indices(n, 1)
+    keep = rng.random(iu[0].size) < density
+    vals = rng.integers(1, magnitude + 1, keep.sum()) * rng.choice([-1.0, 1.0], keep.sum())
+    diag = rng.integers(1, magnitude + 1, n) * rng.choice([-1.0, 1.0], n)
+    return QuboInstance(f"r{seed}", "random", n, diag.astype(float), iu[0][keep], iu[1][keep],
+                        vals.astype(float))
+
+
+@pytest.fixture(scope="module")
+def lib(native):
+    from reformulation_b200.praq import Library
+    return Library()
+
+
+def rel(a, b):
+    return abs(a - b) / (1.0 + abs(b))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8])
+@pytest.mark.parametrize("density", [1.0, 0.5, 0.2, 0.0])
+def test_enumerated_optimum_fp64(lib, oracle_lib, n, density):
+    inst = random_qubo(1000 * n + int(10 * density), n, density)
+    opt = oracle_lib.half_integral_optimum(inst)
+    s = lib.solve(inst, lib.parameters(tolerance=1e-9))
+    assert s.status == 0
+    assert s.gap <= 1e-9
+    assert s.lower <= opt + 1e-9 * (1 + abs(opt)) and s.upper >= opt - 1e-9 * (1 + abs(opt))
+    assert rel(s.upper, opt) <= 1e-7
+    assert np.all((s.x >= 0) & (s.x <= 1))
+    assert abs(oracle_lib.relaxation_value(inst, s.x) - s.upper) <= 1e-9 * (1 + abs(opt))
+
+
+def test_matches_oracle_config_n200(lib, oracle_lib):
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    ref = oracle_lib.praq_solve(inst, oracle_lib.praq_params(tolerance=1e-9))
+    s = lib.solve(inst, lib.parameters(tolerance=1e-9))
+    assert s.status == 0 and ref["status"] == 0
+    assert abs(s.iterations - ref["iterations"]) <= 16
+    assert rel(s.upper, ref["upper"]) <= 1e-8 and rel(s.lower, ref["lower"]) <= 1e-8
+    flow = oracle_lib.roof_dual_maxflow(inst)
+    assert rel(s.upper, flow) <= 1e-7 and s.lower <= flow + 1e-6
+
+
+def test_bounds_bracket_under_every_cap(lib, oracle_lib):
+    inst = random_qubo(101, 8, 0.6)
+    opt = oracle_lib.half_integral_optimum(inst)
+    for cap in (1, 4, 16, 64, 256):
+        s = lib.solve(inst, lib.parameters(tolerance=1e-12, max_iter=cap))
+        assert s.status in (0, 1)
+        assert s.iterations <= cap + 15
+        assert s.lower <= opt + 1e-9 * (1 + abs(opt))
+        assert s.upper >= opt - 1e-9 * (1 + abs(opt))
+        assert s.status == 1 or s.gap <= 1e-12
+
+
+@pytest.mark.parametrize("n", [4, 6, 8])
+def test_float32_accuracy(lib, oracle_lib, n):
+    inst = random_qubo(200 + n, n, 0.7)
+    opt = oracle_lib.half_integral_optimum(inst)
+    s = lib.solve(inst, lib.parameters(tolerance=1e-4, use_float32=1))
+    assert s.status == 0
+    assert rel(s.upper, opt) <= 1e-3 and rel(s.lower, opt) <= 1e-3
+
+
+def test_larger_instance_certifies_itself(lib, oracle_lib):
+    inst = random_qubo(300, 400, 0.05)
+    s = lib.solve(inst, lib.parameters(tolerance=1e-8))
+    assert s.status == 0 and s.gap <= 1e-8
+    f = oracle_lib.relaxation_value(inst, s.x)
+    assert abs(f - s.upper) <= 1e-9 * (1 + abs(f))
+    ref = oracle_lib.praq_solve(inst, oracle_lib.praq_params(tolerance=1e-8))
+    assert abs(s.iterations - ref["iterations"]) <= 16
+    assert rel(s.upper, ref["upper"]) <= 1e-7
+
+
+def test_dual_certificate_recomputed_on_host(native, oracle_lib):
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    p = Library().parameters(tolerance=1e-8)
+    with DeviceSolver(inst, p) as dev:
+        assert dev.run() == 0
+        res, y = dev.result(want_x=True, want_dual=True)
+    # dual feasibility (covering: equal pair in [-w, 0]; packing: a + b = w, both >= 0)
+    w = 2.0 * np.abs(inst.vals)
+    cov = inst.vals > 0
+    assert np.all(np.abs(y[cov, 0] - y[cov, 1]) <= 1e-9 * (1 + w[cov]))
+    assert np.all(y[cov, 0] <= 1e-12) and np.all(y[cov, 0] >= -w[cov] - 1e-9)
+    assert np.all(np.abs(y[~cov].sum(1) - w[~cov]) <= 1e-9 * (1 + w[~cov]))
+    assert np.all(y[~cov] >= -1e-12)
+    low = oracle_lib.qubo_lower_bound(inst, y)
+    assert rel(low, res.lower) <= 1e-9
+    assert rel(oracle_lib.relaxation_value(inst, res.x), res.upper) <= 1e-9
+
+
+def test_deterministic_across_runs(native):
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = random_qubo(7, 300, 0.1)
+    p = Library().parameters(tolerance=1e-8)
+    with DeviceSolver(inst, p) as dev:
+        dev.run()
+        a = dev.result()
+        dev.run()
+        b = dev.result()
+    assert a.iterations == b.iterations
+    assert a.lower == b.lower and a.upper == b.upper
+    assert np.array_equal(a.x, b.x)
+
+
+def test_rejects_bad_input(lib):
+    from reformulation_b200 import _native
+    import ctypes
+    inst = random_qubo(1, 3, 1.0)
+    p = lib.parameters()
+    x = np.empty(3)
+    r = _native.PraqResult()
+    L = _native.lib()
+    assert L.praq_solve(None, ctypes.byref(p), _native.dptr(x), ctypes.byref(r)) == -1
+    bad = QuboInstance("b", "b", 3, inst.diag, inst.rows.copy(), inst.cols.copy(), inst.vals)
+    bad.cols[0] = bad.rows[0]
+    assert lib.solve(bad, p).status == -2
+    bad2 = QuboInstance("b", "b", 3, inst.diag, inst.rows.copy(), inst.cols.copy(), inst.vals)
+    bad2.cols[0] = 3
+    assert lib.solve(bad2, p).status == -2
+    empty = QuboInstance("e", "e", 0, np.zeros(0), np.zeros(0, np.int64), np.zeros(0, np.int64),
+                         np.zeros(0))
+    assert lib.solve(empty, p).status == -2
+    q = lib.parameters(omega=-1.0)
+    assert lib.solve(inst, q).status == -1
+
+
+def test_interval_rule_op_steps_zero(lib):
+    p = lib.parameters()
+    assert lib.check_interval(50_000, lib.parameters(op_steps=0)) == 2
+    inst = random_qubo(3, 60, 1.0)
+    s = lib.solve(inst, lib.parameters(tolerance=1e-8, op_steps=0))
+    assert s.status == 0
+    assert s.iterations % 2 == 0 and s.iterations > 0
+    del p
+
+
+def test_backend_solve_api(native):
+    from reformulation_b200 import praq
+    from reformulation_b200.results import Tolerances
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    r = praq.solve(inst, tolerances=Tolerances(optimality=1e-6), time_limit=60.0)
+    assert r.status == "optimal" and r.objective == r.upper
+    assert r.iterations > 0 and np.isnan(r.feasibility_tolerance)
+    m = praq.solve(inst, tolerances=Tolerances(optimality=1e-4), time_limit=60.0,
+                   precision="mixed")
+    assert m.status == "optimal"
+    assert rel(m.objective, r.objective) <= 1e-3
+    c = praq.solve(inst, tolerances=Tolerances(optimality=1e-12), time_limit=60.0, max_iter=32)
+    assert c.status == "iteration_limit" and np.isnan(c.objective) and c.lower <= c.upper
