@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""bench.py -- solves/s of the restarted Halpern PDHG hot path on B200.
+
+Workload (one "step" = one full solve from the cold start):
+    PRAQ, the QUBO roof-dual LP of a graph with n = 100,000 nodes and
+    m = 1,000,000 distinct uniform pairs (seed 1), integer weights in
+    [-100, 100], solved to 1e-4 relative gap (= relative KKT: both iterates
+    are feasible by construction), FP32 iterates with FP64 reductions /
+    restart logic / bounds ("mixed").  The plain FP64 kernel on the same
+    instance is timed beside it.
+
+Timing: W untimed warm-up solves, then exactly K timed solves, each between a
+CUDA event pair on the solver's stream (torch's current stream, passed down the
+C ABI), with L2 flushed (a 256 MB write) before every solve and outside the
+event pair; barrier + synchronize on both sides; max over ranks.  `value` is
+whole-job solves/s.  `e2e` is the same metric through the reference-facing C
+call praq_solve with host buffers (host layout build, host->device upload and
+device->host result inside the timed region).
+
+Multi-GPU: PRAQ instances are independent, so N GPUs run N replicas (weak
+scaling, no collective on the data path); torch.distributed/NCCL only carries
+the barrier and the max-over-ranks reduction of the timings.
+
+--impl reference: the reference's CPU implementation of this path is its JAX
+specification, which cannot run here (no jax); the arm times the CPU
+restatement of it (oracle/praq_oracle.c, all host threads) on the same
+workload, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "solves/sec and p50/p99 latency at 1e-4 rel KKT vs plain FP64 PDHG, 1 B200"
+UNIT = "solves/s"
+TOL = 1e-4
+N_NODES, N_EDGES, SEED = 100_000, 1_000_000, 1
+WORKLOAD = ("PRAQ QUBO roof-dual LP, n=100000 nodes, m=1000000 uniform distinct pairs "
+            "(seed 1), weights U{-100..100}, solve to 1e-4 relative gap")
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(n: int, m: int, real: int, index: int = 4) -> dict:
+    """Per-launch algorithmic bytes of the two step kernels.  The per-iteration
+    total is the PRAQ figure n (6R + I) + m (11R + 4I): the node kernel reads
+    x (predicted), x0, diag, deg and the CSR pointer and writes x, r
+    (n (6R + I)) and reads the CSR index and one gathered dual per half-edge
+    (m (2I + 2R)); the edge kernel reads both ends, the weight, the predicted
+    dual pair, the anchor pair and r at both ends and writes the dual pair
+    (m (2I + 9R))."""
+    node = n * (6 * real + index) + m * (2 * index + 2 * real)
+    edge = m * (2 * index + 9 * real)
+    return {"node": node, "edge": edge, "node_check": node, "edge_check": edge,
+            "iteration": node + edge}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms into a file."""
+
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self, bus_id: str | None):
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            if bus_id and bus_id.lower() not in parts[0].lower() and parts[0].lower() not in bus_id.lower():
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), max=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], pcap=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [r for r in rows if r["power"] > 200.0] or rows
+        reasons = set()
+        for r in loaded:
+            if r["hw"] == "Active":
+                reasons.add("hw_slowdown")
+            if r["hwt"] == "Active":
+                reasons.add("hw_thermal_slowdown")
+            if r["swt"] == "Active":
+                reasons.add("sw_thermal_slowdown")
+            if r["pcap"] == "Active":
+                reasons.add("sw_power_cap")
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded),
+                "sm_max_mhz": max(r["max"] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows), "samples_under_load": len(loaded)}
+
+
+def read_traffic(kind: str):
+    """dram bytes per launch of `kind` from the committed ncu summary, if any."""
+    path = ROOT / "profiles" / "praq_kernels_n100k_m1M.txt"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kind:
+            return float(parts[2])
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0))
+
+
+def cpu_leg(inst, threads: int, budget_s: float = 20.0, max_solves: int = 20):
+    """The oracle (CPU restatement of the reference's JAX solver), FP64, full
+    solves to 1e-4 until `budget_s` of CPU time or `max_solves`."""
+    import oracle
+    p = oracle.praq_params(tolerance=TOL)
+    times, iters = [], []
+    t_begin = time.perf_counter()
+    while len(times) < max_solves and (time.perf_counter() - t_begin) < budget_s:
+        t0 = time.perf_counter()
+        r = oracle.praq_solve(inst, p, threads=threads)
+        times.append(time.perf_counter() - t0)
+        iters.append(r["iterations"])
+    return times, iters
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from reformulation_b200.instances import qubo_uniform_edges
+    inst = qubo_uniform_edges(SEED, N_NODES, N_EDGES)
+    threads = cpu_threads()
+    # warm-up: page in the oracle and the instance
+    cpu_leg(inst, threads, budget_s=0.0, max_solves=max(1, min(args.warmup, 1)))
+    times, iters = cpu_leg(inst, threads, budget_s=1e9, max_solves=args.steps)
+    total = sum(times)
+    value = len(times) / total
+    sample = (f"{len(times)} full solves of the workload to 1e-4 (FP64, {iters[0]} iterations), "
+              f"CPU restatement oracle/praq_oracle.c with {threads} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64 (CPU)", "l2": "n/a (CPU)"},
+        "p50_ms": 1e3 * float(np.percentile(times, 50)), "p99_ms": 1e3 * float(np.percentile(times, 99)),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference's CPU implementation of this path is its JAX solver "
+                 "(qubo/praq-jax), which cannot run without jax; this arm times the CPU "
+                 "restatement of it"),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def time_solves(dev, steps, flush, torch, stream):
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    launches = 0
+    statuses = []
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        statuses.append(dev.run())
+        ends[k].record(stream)
+        launches += dev.launches()
+    torch.cuda.synchronize()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    return ms, launches, statuses
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from reformulation_b200 import build as native_build
+    from reformulation_b200 import praq
+    from reformulation_b200.instances import qubo_uniform_edges
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    native_build.build()
+    stream = torch.cuda.current_stream(device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    inst = qubo_uniform_edges(SEED, N_NODES, N_EDGES)
+    lib = praq.Library()
+    p_mixed = lib.parameters(tolerance=TOL, use_float32=1, max_iter=1_000_000)
+    p_fp64 = lib.parameters(tolerance=TOL, use_float32=0, max_iter=1_000_000)
+    mixed = praq.DeviceSolver(inst, p_mixed, stream=stream.cuda_stream)
+    fp64 = praq.DeviceSolver(inst, p_fp64, stream=stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    for _ in range(args.warmup):
+        mixed.run()
+        fp64.run()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler()
+    if rank == 0:
+        sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    ms, launches, statuses = time_solves(mixed, args.steps, flush, torch, stream)
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - wall0
+    if rank == 0:
+        sampler.stop()
+    res = mixed.result()
+    total_ms = max_over_ranks(sum(ms))
+    value = world * args.steps / (total_ms / 1e3)
+
+    # the plain FP64 kernel on the same instance, same protocol
+    barrier()
+    ms64, _, st64 = time_solves(fp64, args.steps, flush, torch, stream)
+    barrier()
+    res64 = fp64.result()
+    total64 = max_over_ranks(sum(ms64))
+    value64 = world * args.steps / (total64 / 1e3)
+
+    # live per-kernel timing (event pair around every launch of one solve)
+    _, prof = mixed.run_profiled()
+    kinds = {k: v for k, v in prof.items() if v[1] > 0}
+    dominant = max(kinds, key=lambda k: kinds[k][0])
+    per_launch_ms = kinds[dominant][0] / kinds[dominant][1]
+    alg = algorithmic_bytes(N_NODES, N_EDGES, 4)
+    hbm_peak, peak_kind = peaks()
+    achieved = alg.get(dominant, 0) / (per_launch_ms / 1e3) / 1e9
+    _, prof64 = fp64.run_profiled()
+    alg64 = algorithmic_bytes(N_NODES, N_EDGES, 8)
+
+    # e2e through the reference-facing C call, host buffers
+    barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s = lib.solve(inst, p_mixed)
+        e2e_times.append(time.perf_counter() - t0)
+        assert s.status == 0
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_times))
+    e2e_value = world * args.steps / e2e_total
+    n, m = N_NODES, N_EDGES
+    h2d = 2 * (n + 1) * 4 + m * 4 + m * 8 + m * 4 + 3 * n * 4
+    blocks = res.iterations // 16 + 2
+    d2h = n * 4 + 96 * (blocks + 2)
+
+    line = None
+    if rank == 0:
+        clocks = sampler.summary(torch.cuda.get_device_properties(device).pci_bus_id
+                                 if hasattr(torch.cuda.get_device_properties(device), "pci_bus_id")
+                                 else None)
+        lat = np.array(ms)
+        lat64 = np.array(ms64)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 iterates, f64 reductions", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "mixed (fp32 iterates / fp64 reductions)",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "flushed before every solve (256 MB write, outside the timed events)"},
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "iterations": res.iterations, "relative_gap": res.gap, "lower": res.lower,
+            "upper": res.upper, "statuses_ok": all(s == 0 for s in statuses),
+            "plain_fp64": {"value": value64, "unit": UNIT, "ms_per_step": total64 / args.steps,
+                           "p50_ms": float(np.percentile(lat64, 50)),
+                           "p99_ms": float(np.percentile(lat64, 99)),
+                           "iterations": res64.iterations, "relative_gap": res64.gap,
+                           "upper": res64.upper,
+                           "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in prof64.items() if v[1]},
+                           "edge_kernel_gbs": alg64["edge"] / (prof64["edge"][0] / prof64["edge"][1] / 1e3) / 1e9},
+            "mixed_vs_fp64": value / value64,
+            "roofline": {"bound": "hbm", "kernel": f"praq {dominant} kernel (fp32)",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                         "frac_of_8tbs": achieved / 8000.0,
+                         "algorithmic_bytes_per_launch": alg.get(dominant),
+                         "avg_launch_us": per_launch_ms * 1e3,
+                         "traffic": read_traffic(dominant)},
+            "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in kinds.items()},
+            "kernels_share": {k: v[0] / sum(x[0] for x in kinds.values()) for k, v in kinds.items()},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "p50_ms": 1e3 * float(np.percentile(e2e_times, 50))},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+
+    # CPU baseline and the reference's own praq-cuda, rank 0 at N=1 only
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        threads = cpu_threads()
+        times, iters = cpu_leg(inst, threads, budget_s=20.0, max_solves=10)
+        line["cpu_baseline"] = {
+            "value": len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"{len(times)} full FP64 solves of the workload to 1e-4 ({iters[0]} "
+                       f"iterations each) by the CPU restatement oracle/praq_oracle.c, "
+                       f"{threads} OpenMP threads")}
+        try:
+            import oracle
+            rp = oracle.RefPraq()
+            ref_rows = {}
+            for prec in (0, 1):
+                rp.solve(inst, tolerance=TOL, use_float32=prec)
+                tt = []
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    rr = rp.solve(inst, tolerance=TOL, use_float32=prec)
+                    tt.append(time.perf_counter() - t0)
+                ref_rows["f32" if prec else "f64"] = {
+                    "solves_per_s_e2e": 3 / sum(tt), "iterations": rr["iterations"],
+                    "upper": rr["upper"]}
+            line["reference_praq_cuda_same_gpu"] = ref_rows
+        except Exception as exc:  # the reference build is optional context
+            line["reference_praq_cuda_same_gpu"] = {"unavailable": str(exc)[:120]}
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    fp64.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -114,6 +114,14 @@ REFORM_API int reform_praq_result(reform_praq_solver* solver, double* x, double*
 #define PRAQ_STATUS_TIME_LIMIT 2
 REFORM_API int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds);
 
+/* A measurement run: the same solve with every kernel launched on its own
+ * between a pair of CUDA events on the solver's stream.  ms[9] and count[9]
+ * receive each kernel kind's total device milliseconds and launch count, in
+ * this order: node step, edge step, node step with check sums, edge step with
+ * check sums, lower-bound pass, check, restart node step, restart edge step,
+ * restart check.  Returns the status like reform_praq_run. */
+REFORM_API int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* count);
+
 /* Kernel launches the last run issued (graph kernel nodes included). */
 REFORM_API int64_t reform_praq_launches(const reform_praq_solver* solver);
 

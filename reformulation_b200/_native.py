@@ -70,6 +70,7 @@ def _declare(lib):
         "reform_praq_run": (I, [c_void_p]),
         "reform_praq_result": (I, [c_void_p, D, D, P(PraqResult)]),
         "reform_praq_set_time_limit": (I, [c_void_p, c_double]),
+        "reform_praq_run_profiled": (I, [c_void_p, D, P(c_int64)]),
         "reform_praq_launches": (c_int64, [c_void_p]),
         "reform_praq_destroy": (None, [c_void_p]),
     }

@@ -427,6 +427,7 @@ struct SolverBase {
     virtual int run() = 0;
     virtual int result(double* x, double* y2, PraqResult* r) = 0;
     virtual long long launches() const = 0;
+    virtual int run_profiled(double* ms, long long* count) = 0;
     double time_limit = -1.0;   // seconds of wall clock per run; < 0: none
 };
 
@@ -456,6 +457,7 @@ struct Solver final : SolverBase {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         for (auto& ev : done) if (ev) cudaEventDestroy(ev);
+        for (auto& ev : evpool) cudaEventDestroy(ev);
         row_ptr.release(); col_ptr.release(); col_idx.release(); ends.release();
         w.release(); diag.release(); deg.release(); cpack.release();
         x1.release(); x2.release(); x0.release(); r.release(); pred.release(); u0.release();
@@ -524,26 +526,94 @@ struct Solver final : SolverBase {
     // One op_steps block: op_steps reflected steps (the last with the check
     // sums), the lower-bound pass, the check, then the restart step (gated on
     // the device flag), its error, and a copy of the control block to the host.
+    // Profiled launches: an event pair around every kernel, by kind
+    // (0 node, 1 edge, 2 node+check, 3 edge+check, 4 lower, 5 check,
+    // 6 restart node, 7 restart edge, 8 restart check).
+    static constexpr int kKinds = 9;
+    std::vector<cudaEvent_t> evpool;
+    std::vector<std::pair<int, int>> marks;   // (kind, first event index)
+    bool profiling = false;
+
+    cudaError_t mark_begin(int kind) {
+        if (!profiling) return cudaSuccess;
+        const int idx = int(marks.size()) * 2;
+        while (int(evpool.size()) < idx + 2) {
+            cudaEvent_t ev;
+            RB_CUDA_TRY(cudaEventCreate(&ev));
+            evpool.push_back(ev);
+        }
+        marks.emplace_back(kind, idx);
+        return cudaEventRecord(evpool[idx], stream);
+    }
+    cudaError_t mark_end() {
+        if (!profiling) return cudaSuccess;
+        return cudaEventRecord(evpool[marks.back().second + 1], stream);
+    }
+
+#define RB_TIMED(kind, launch)               \
+    do {                                     \
+        RB_CUDA_TRY(mark_begin(kind));       \
+        launch;                              \
+        RB_CUDA_TRY(mark_end());             \
+    } while (0)
+
+    // One op_steps block: op_steps reflected steps (the last with the check
+    // sums), the lower-bound pass, the check, then the restart step (gated on
+    // the device flag), its error, and a copy of the control block to the host.
     cudaError_t enqueue_block() {
         const int op = int(p.op_steps);
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
-                node_kernel<Real, true, false><<<nb_node, kBlock, 0, stream>>>(d, nullptr, s, 0, 0);
-                if (L.m) edge_kernel<Real, true, false><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0);
+                RB_TIMED(0, (node_kernel<Real, true, false><<<nb_node, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
+                if (L.m) RB_TIMED(1, (edge_kernel<Real, true, false><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
             } else {
-                node_kernel<Real, true, true><<<nb_node, kBlock, 0, stream>>>(d, nullptr, s, 0, 0);
-                if (L.m) edge_kernel<Real, true, true><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0);
+                RB_TIMED(2, (node_kernel<Real, true, true><<<nb_node, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
+                if (L.m) RB_TIMED(3, (edge_kernel<Real, true, true><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
             }
         }
-        lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.u2s);
-        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.pnode, nb_node, d.pedge, nb_edge,
-                                                   d.plower, nb_node, 1);
-        node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1);
-        if (L.m) edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1);
-        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.pnode, nb_node, d.pedge, nb_edge,
-                                                   d.plower, nb_node, 2);
+        RB_TIMED(4, (lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.u2s)));
+        RB_TIMED(5, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.pnode, nb_node, d.pedge,
+                                                                nb_edge, d.plower, nb_node, 1)));
+        RB_TIMED(6, (node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1)));
+        if (L.m) RB_TIMED(7, (edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1)));
+        RB_TIMED(8, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.pnode, nb_node, d.pedge,
+                                                                nb_edge, d.plower, nb_node, 2)));
         RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
         return cudaGetLastError();
+    }
+
+    // A solve with every kernel launched on its own (no graph) between an
+    // event pair; adds each kind's total milliseconds and launch count into
+    // ms[kKinds], count[kKinds].  A measurement mode: same arithmetic, the
+    // host waits after every block.
+    int run_profiled(double* ms, long long* count) override {
+        for (int k = 0; k < kKinds; ++k) { ms[k] = 0.0; count[k] = 0; }
+        int st = start_solve();
+        if (st) return st;
+        profiling = true;
+        while (!mirror->terminated) {
+            marks.clear();
+            if (enqueue_block() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
+                profiling = false;
+                return PRAQ_ERROR_CUDA;
+            }
+            nlaunch += block_nodes;
+            for (auto& mk : marks) {
+                float t = 0.f;
+                if (cudaEventElapsedTime(&t, evpool[mk.second], evpool[mk.second + 1]) != cudaSuccess) {
+                    profiling = false;
+                    return PRAQ_ERROR_CUDA;
+                }
+                ms[mk.first] += t;
+                count[mk.first] += 1;
+            }
+        }
+        profiling = false;
+        if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return PRAQ_ERROR_CUDA;
+        status_override = -100;
+        return mirror->gap <= p.tolerance ? 0 : 1;
     }
 
     cudaError_t capture_block() {
@@ -558,10 +628,9 @@ struct Solver final : SolverBase {
         return cudaSuccess;
     }
 
-    int run() override {
+    // Cold start, the first vanilla step and the check before the loop.
+    int start_solve() {
         nlaunch = 0;
-        const auto started = std::chrono::steady_clock::now();
-        bool timed_out = false;
         const int count = std::max(L.n, L.m);
         init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega,
                                                                            p.theta_initial);
@@ -577,6 +646,17 @@ struct Solver final : SolverBase {
         nlaunch += 4 + (L.m ? 1 : 0);
         if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess)
             return PRAQ_ERROR_CUDA;
+        return 0;
+    }
+
+    int run() override {
+        nlaunch = 0;
+        const auto started = std::chrono::steady_clock::now();
+        bool timed_out = false;
+        {
+            const int st = start_solve();
+            if (st) return st;
+        }
         // Keep one block in flight ahead of the one being inspected; blocks
         // launched after termination see the flag and return at once.
         int inflight = 0;
@@ -740,6 +820,14 @@ int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds) {
     if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
     solver->impl->time_limit = seconds;
     return 0;
+}
+
+int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* count) {
+    if (!solver || !solver->impl || !ms || !count) return PRAQ_ERROR_ARGUMENT;
+    long long c[9];
+    const int st = solver->impl->run_profiled(ms, c);
+    for (int k = 0; k < 9; ++k) count[k] = c[k];
+    return st;
 }
 
 int64_t reform_praq_launches(const reform_praq_solver* solver) {

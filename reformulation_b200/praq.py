@@ -131,6 +131,18 @@ class DeviceSolver:
     def launches(self) -> int:
         return int(self._lib.reform_praq_launches(self._h))
 
+    #: kernel kinds of `run_profiled`, in the order the C ABI reports them
+    KINDS = ("node", "edge", "node_check", "edge_check", "lower", "check",
+             "restart_node", "restart_edge", "restart_check")
+
+    def run_profiled(self) -> tuple[int, dict]:
+        """A solve with an event pair around every kernel launch; returns the
+        status and {kind: (total_ms, launches)}."""
+        ms = np.zeros(len(self.KINDS))
+        count = np.zeros(len(self.KINDS), dtype=np.int64)
+        st = self._lib.reform_praq_run_profiled(self._h, _native.dptr(ms), _native.iptr(count))
+        return int(st), {k: (float(ms[i]), int(count[i])) for i, k in enumerate(self.KINDS)}
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.reform_praq_destroy(self._h)
