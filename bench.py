@@ -316,9 +316,11 @@ def run_ours(args):
 
     line = None
     if rank == 0:
-        clocks = sampler.summary(torch.cuda.get_device_properties(device).pci_bus_id
-                                 if hasattr(torch.cuda.get_device_properties(device), "pci_bus_id")
-                                 else None)
+        props = torch.cuda.get_device_properties(device)
+        bus = None
+        if all(hasattr(props, a) for a in ("pci_domain_id", "pci_bus_id", "pci_device_id")):
+            bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}"
+        clocks = sampler.summary(bus)
         lat = np.array(ms)
         lat64 = np.array(ms64)
         line = {

@@ -1,0 +1,48 @@
+// memory.cuh -- device and pinned-host memory for the solvers.
+//
+// Device memory comes from one library-owned stream-ordered pool per device
+// (cudaMemPoolCreate) whose release threshold keeps freed blocks cached for
+// the next solve, so a one-shot solve pays no cudaMalloc.  Control-block
+// mirrors come from one pinned-host slab carved into 256-byte slots.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "common.cuh"
+
+namespace rb200 {
+
+cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
+void* pinned_get();          // a 256-byte pinned slot, or nullptr
+void pinned_put(void* slot);
+
+template <class T>
+struct PoolBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaStream_t stream = nullptr;
+    PoolBuf() = default;
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    ~PoolBuf() { release(); }
+    void release() {
+        if (ptr) cudaFreeAsync(ptr, stream);
+        ptr = nullptr;
+        count = 0;
+    }
+    cudaError_t alloc(size_t n, cudaStream_t s) {
+        release();
+        stream = s;
+        count = n;
+        return pool_alloc(reinterpret_cast<void**>(&ptr), sizeof(T) * n, s);
+    }
+    cudaError_t upload(const T* host, size_t n, cudaStream_t s) {
+        RB_CUDA_TRY(alloc(n, s));
+        if (n) RB_CUDA_TRY(cudaMemcpyAsync(ptr, host, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+        return cudaSuccess;
+    }
+};
+
+}  // namespace rb200

@@ -178,3 +178,27 @@ def test_backend_solve_api(native):
     assert rel(m.objective, r.objective) <= 1e-3
     c = praq.solve(inst, tolerances=Tolerances(optimality=1e-12), time_limit=60.0, max_iter=32)
     assert c.status == "iteration_limit" and np.isnan(c.objective) and c.lower <= c.upper
+
+
+def test_unsorted_and_reversed_edges(lib, oracle_lib):
+    """Edges in any order and either orientation: the device layout sorts
+    them; the optimum and the returned primal do not depend on the order."""
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    rng = np.random.default_rng(9)
+    order = rng.permutation(inst.edges)
+    flip = rng.random(inst.edges) < 0.5
+    rows, cols = inst.rows[order].copy(), inst.cols[order].copy()
+    rows[flip], cols[flip] = cols[flip], rows[flip].copy()
+    shuffled = QuboInstance("s", "s", inst.n, inst.diag, rows, cols, inst.vals[order])
+    a = lib.solve(inst, lib.parameters(tolerance=1e-9))
+    b = lib.solve(shuffled, lib.parameters(tolerance=1e-9))
+    flow = oracle_lib.roof_dual_maxflow(inst)
+    assert a.status == 0 and b.status == 0
+    assert rel(a.upper, flow) <= 1e-7 and rel(b.upper, flow) <= 1e-7
+    assert abs(oracle_lib.relaxation_value(inst, b.x) - b.upper) <= 1e-9 * (1 + abs(flow))
+    from reformulation_b200.praq import DeviceSolver
+    with DeviceSolver(shuffled, lib.parameters(tolerance=1e-8)) as dev:
+        dev.run()
+        res, y = dev.result(want_dual=True)
+    low = oracle_lib.qubo_lower_bound(shuffled, y)
+    assert rel(low, res.lower) <= 1e-9
