@@ -127,6 +127,36 @@ REFORM_API int64_t reform_praq_launches(const reform_praq_solver* solver);
 
 REFORM_API void reform_praq_destroy(reform_praq_solver* solver);
 
+/* ---- the bracket of a given point, with no device allocation ------------- */
+
+/* No counterpart in the reference.  The roof-dual bracket of a primal-dual
+ * pair, lower = L_D(y) and upper = F(x) in the instance's own units (the
+ * reference's relaxation_bounds, qubo/praq-jax/praq/solver.py:348-362), for
+ * callers that cannot allocate device memory where they need it: code running
+ * inside its own stream capture (allocation is not capturable), real-time
+ * loops that must not touch the allocator, and frameworks that own all device
+ * memory and hand a library only buffers.
+ *
+ * Every pointer is DEVICE memory the caller owns: diag [n], rows/cols [m]
+ * (int64), vals [m], x [n], y [2m] (half-edge pairs), out [2] = (lower, upper).
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = the legacy stream)
+ * and is complete when that stream is; the call itself does not synchronise.
+ *
+ * The scratch is one fixed file-scope device array of 262,144 + 1,185 doubles
+ * (about 2 MiB), held by every GPU that loads the library until the process
+ * exits.  Limits: 1 <= n <= 262,144 (PRAQ_ERROR_INSTANCE beyond it), any m.
+ * The first call on a device looks up the array's device address (with that
+ * device current) and caches it: make that first call before any stream
+ * capture.  Calls share the array, so calls whose work overlaps on the GPU
+ * (two streams, or two threads) race and give wrong results; serialise them.
+ * An out-of-range edge index is skipped and both outputs become NaN.
+ * Returns 0, PRAQ_ERROR_ARGUMENT for a null pointer, PRAQ_ERROR_INSTANCE for
+ * n or m out of range, PRAQ_ERROR_CUDA if the launch failed. */
+REFORM_API int reform_praq_bounds_noalloc(int64_t n, int64_t m, const double* diag,
+                                          const int64_t* rows, const int64_t* cols,
+                                          const double* vals, const double* x,
+                                          const double* y, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

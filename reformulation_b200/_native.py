@@ -73,6 +73,8 @@ def _declare(lib):
         "reform_praq_run_profiled": (I, [c_void_p, D, P(c_int64)]),
         "reform_praq_launches": (c_int64, [c_void_p]),
         "reform_praq_destroy": (None, [c_void_p]),
+        "reform_praq_bounds_noalloc": (I, [c_int64, c_int64, c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
