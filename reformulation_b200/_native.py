@@ -76,6 +76,27 @@ def _declare(lib):
         "reform_praq_bounds_noalloc": (I, [c_int64, c_int64, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     }
+    F = POINTER(ctypes.c_float)
+    sig.update({
+        "pria_params_auto": (PriaParams, [c_int64, c_double]),
+        "pria_solve_f64": (I, [c_int64, c_int64, D, c_double, D, P(PriaParams), D, D, D, D, D, D,
+                               P(PriaResultInfo)]),
+        "pria_solve_f32": (I, [c_int64, c_int64, F, ctypes.c_float, F, P(PriaParams), F, F, F, F, F,
+                               F, P(PriaResultInfo)]),
+        "pria_solve_batch_f64": (I, [c_int64, c_int64, c_int64, D, D, D, P(PriaParams), D, D, D,
+                                     P(PriaResultInfo)]),
+        "pria_solve_batch_f32": (I, [c_int64, c_int64, c_int64, F, F, F, P(PriaParams), F, F, F,
+                                     P(PriaResultInfo)]),
+        "pria_objective_f64": (c_double, [c_int64, c_int64, D, c_double, D, D]),
+        "reform_pria_create": (I, [c_int64, c_int64, D, c_double, D, P(PriaParams), I, c_void_p,
+                                   P(c_void_p)]),
+        "reform_pria_run": (I, [c_void_p]),
+        "reform_pria_set_warm": (I, [c_void_p, D, D, D]),
+        "reform_pria_result": (I, [c_void_p, D, D, D, P(PriaResultInfo)]),
+        "reform_pria_run_profiled": (I, [c_void_p, D, P(c_int64)]),
+        "reform_pria_launches": (c_int64, [c_void_p]),
+        "reform_pria_destroy": (None, [c_void_p]),
+    })
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res
@@ -97,6 +118,10 @@ def lib():
 
 def dptr(a):
     return a.ctypes.data_as(POINTER(c_double))
+
+
+def fptr(a):
+    return a.ctypes.data_as(POINTER(ctypes.c_float))
 
 
 def iptr(a):

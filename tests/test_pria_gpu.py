@@ -1,0 +1,166 @@
+"""PRIA on the GPU against the oracles, through the C ABI.
+
+Patterned on the reference's checks (jrp/pria-cuda/tests/test_solver.cu:37-389,
+jrp/pria-jax/tests/test_solver.py:51-187): agreement with the reference's own
+CPU solver ref::solve (iterations within one check interval, bounds), the HiGHS
+optimum of the golden fixtures, a certificate recomputed on the host (primal
+objective of the returned x, dual bound of the returned normalised y and z,
+feasibility of all three), FP32 accuracy, the warm-start fixed point (even T:
+zero iterations), odd-T padding, batch = solo, bad inputs, determinism.
+
+Tolerances: FP64 bounds within 1e-6 relative of ref::solve's at the same
+tolerance (different summation order: sort-based vs Michelot thresholds can
+move a check by one block, so iterations within +-op_steps); objective within
+10 x the solve tolerance of HiGHS; FP32 within 1e-3 relative of FP64.
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from reformulation_b200.instances import JrpInstance, jrp_demand
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def rel(a, b):
+    return abs(a - b) / (1.0 + abs(b))
+
+
+def jrp_from(rec):
+    n, t = rec["n"], rec["t"]
+    return JrpInstance(rec["name"], "golden", np.array(rec["k"], float), rec["k0"],
+                       np.array(rec["h"], float).reshape(n, t, t))
+
+
+@pytest.fixture(scope="module")
+def lib(native):
+    from reformulation_b200.pria import Library
+    return Library()
+
+
+def feasible(inst, s, tol=1e-9):
+    x, y, z = s.x, s.y, s.z
+    n, t = inst.items, inst.periods
+    upper = np.triu(np.ones((t, t), bool))
+    assert np.all(x >= -tol) and np.all(y >= -tol) and np.all(z >= -tol)
+    assert np.all(x[:, ~upper] == 0) and np.all(y[:, ~upper] == 0)
+    assert np.allclose(x.sum(axis=1), 1.0, atol=1e-7)          # sum_{s<=t} x = 1
+    ok = inst.order_costs > 0
+    assert np.allclose(y[ok].sum(axis=2), 1.0, atol=1e-7)      # rows sum to 1 (normalised)
+    if inst.joint_order_cost > 0:
+        assert np.allclose(z.sum(axis=(0, 2)), 1.0, atol=1e-7)  # groups sum to 1
+
+
+@pytest.mark.parametrize("rec", json.loads((GOLDEN / "pria_golden.json").read_text())["instances"],
+                         ids=lambda r: r["name"])
+def test_golden_against_reference_and_highs(lib, oracle_lib, rec):
+    inst = jrp_from(rec)
+    s = lib.solve(inst, lib.parameters(-1, rec["tol"]), want_solution=True)
+    assert s.status == 0
+    assert abs(s.iterations - rec["ref_iterations"]) <= 16
+    assert rel(s.dual_objective, rec["ref_dual"]) <= 1e-6
+    assert rel(s.primal_objective, rec["highs"]) <= 10 * rec["tol"]
+    assert s.dual_objective <= rec["highs"] + 1e-7 * (1 + abs(rec["highs"]))
+    feasible(inst, s)
+    assert rel(oracle_lib.pria_objective(inst, s.x), s.primal_objective) <= 1e-12
+    assert oracle_lib.pria_dual_bound(inst, s.y, s.z) <= rec["highs"] + 1e-7 * (1 + abs(rec["highs"]))
+
+
+@pytest.mark.parametrize("shape", [(3, 10, 25), (7, 8, 21), (9, 20, 50)])
+def test_matches_reference_cpu_solver(lib, oracle_lib, shape):
+    seed, n, t = shape
+    inst = oracle_lib.ref_pria_random_instance(seed, n, t) if seed != 7 else jrp_demand(seed, n, t)
+    p = oracle_lib.pria_params(tolerance=1e-6)
+    ref = oracle_lib.ref_pria_solve(inst, p)
+    s = lib.solve(inst, lib.parameters(-1, 1e-6), want_solution=True)
+    assert s.status == 0 and s.relative_gap <= 1e-6
+    assert abs(s.iterations - ref["iterations"]) <= 16
+    assert rel(s.dual_objective, ref["lower"]) <= 1e-6
+    assert rel(s.primal_objective, ref["upper"]) <= 1e-5
+    feasible(inst, s)
+
+
+def test_float32_accuracy(lib):
+    inst = jrp_demand(11, 12, 40)
+    a = lib.solve(inst, lib.parameters(-1, 1e-6))
+    b = lib.solve(inst, lib.parameters(-1, 1e-4), precision="mixed", want_solution=True)
+    assert b.status == 0 and b.relative_gap <= 1e-4
+    assert rel(b.primal_objective, a.primal_objective) <= 1e-3
+    assert b.x.dtype == np.float32
+
+
+def test_warm_start_is_a_fixed_point(lib):
+    inst = jrp_demand(12, 6, 20)             # even T: nothing padded
+    s = lib.solve(inst, lib.parameters(-1, 1e-8), want_solution=True)
+    w = lib.solve(inst, lib.parameters(-1, 1e-8), want_solution=True, warm=(s.x, s.y, s.z))
+    assert w.status == 0
+    assert w.iterations == 0
+    assert rel(w.primal_objective, s.primal_objective) <= 1e-9
+
+
+def test_odd_periods_are_padded(lib, oracle_lib):
+    inst = jrp_demand(13, 5, 17)
+    s = lib.solve(inst, lib.parameters(-1, 1e-7), want_solution=True)
+    assert s.status == 0 and s.relative_gap <= 1e-7
+    assert s.x.shape == (5, 17, 17)
+    feasible(inst, s)
+    ref = oracle_lib.pria_solve(inst, oracle_lib.pria_params(tolerance=1e-7))
+    assert rel(s.primal_objective, ref["upper"]) <= 1e-6
+
+
+def test_batch_equals_solo(native, lib):
+    import ctypes
+
+    from reformulation_b200 import _native
+    insts = [jrp_demand(20 + b, 4, 12) for b in range(3)]
+    n, t = 4, 12
+    k = np.concatenate([i.order_costs for i in insts])
+    k0 = np.array([i.joint_order_cost for i in insts])
+    h = np.concatenate([i.holding_costs.ravel() for i in insts])
+    x = np.empty(3 * n * t * t)
+    infos = (_native.PriaResultInfo * 3)()
+    p = lib.parameters(-1, 1e-7)
+    st = _native.lib().pria_solve_batch_f64(3, n, t, _native.dptr(k), _native.dptr(k0), _native.dptr(h),
+                                             ctypes.byref(p), _native.dptr(x), None, None, infos)
+    assert st == 0
+    for b, inst in enumerate(insts):
+        s = lib.solve(inst, p, want_solution=True)
+        assert infos[b].iterations == s.iterations
+        assert infos[b].primal_objective == s.primal_objective
+        assert np.array_equal(x[b * n * t * t:(b + 1) * n * t * t].reshape(n, t, t), s.x)
+
+
+def test_rejects_bad_input(lib):
+    inst = jrp_demand(1, 2, 4)
+    bad = JrpInstance("b", "b", np.zeros(0), 1.0, np.zeros((0, 4, 4)))
+    assert lib.solve(bad, lib.parameters()).status != 0
+    big = JrpInstance("b", "b", np.ones(1), 1.0, np.zeros((1, 1030, 1030)))
+    assert lib.solve(big, lib.parameters()).status != 0
+    assert lib.solve(inst, lib.parameters()).status == 0
+
+
+def test_max_iter_is_exact(lib):
+    inst = jrp_demand(5, 10, 30)
+    s = lib.solve(inst, lib.parameters(64, 1e-12))
+    assert s.status == 0 and s.iterations == 64
+
+
+def test_deterministic_and_backend(native):
+    from reformulation_b200 import pria
+    from reformulation_b200.results import Tolerances
+    inst = jrp_demand(4, 15, 60)
+    with pria.DeviceSolver(inst, pria.Library().parameters(-1, 1e-6)) as dev:
+        dev.run()
+        a = dev.result(want_solution=True)
+        dev.run()
+        b = dev.result(want_solution=True)
+    assert a.iterations == b.iterations and a.primal_objective == b.primal_objective
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.z, b.z)
+    r = pria.solve(inst, tolerances=Tolerances(optimality=1e-6), time_limit=60.0)
+    assert r.status == "optimal" and r.objective == r.upper and r.entries == inst.entries
+    m = pria.solve(inst, tolerances=Tolerances(optimality=1e-4), time_limit=60.0, precision="mixed")
+    assert m.status == "optimal" and rel(m.objective, r.objective) <= 1e-3
