@@ -50,9 +50,16 @@ def feasible(inst, s, tol=1e-9):
     assert np.all(x[:, ~upper] == 0) and np.all(y[:, ~upper] == 0)
     assert np.allclose(x.sum(axis=1), 1.0, atol=1e-7)          # sum_{s<=t} x = 1
     ok = inst.order_costs > 0
-    assert np.allclose(y[ok].sum(axis=2), 1.0, atol=1e-7)      # rows sum to 1 (normalised)
-    if inst.joint_order_cost > 0:
-        assert np.allclose(z.sum(axis=(0, 2)), 1.0, atol=1e-7)  # groups sum to 1
+    # normalised duals: rows of y and groups of z sum to 1 on the padded
+    # problem; an odd T drops the pad period from the output, so there they
+    # sum to at most 1 (the dropped mass is nonnegative)
+    ysum, zsum = y[ok].sum(axis=2), z.sum(axis=(0, 2))
+    if t % 2 == 0:
+        assert np.allclose(ysum, 1.0, atol=1e-7)
+        if inst.joint_order_cost > 0:
+            assert np.allclose(zsum, 1.0, atol=1e-7)
+    else:
+        assert np.all(ysum <= 1.0 + 1e-7) and np.all(zsum <= 1.0 + 1e-7)
 
 
 @pytest.mark.parametrize("rec", json.loads((GOLDEN / "pria_golden.json").read_text())["instances"],
