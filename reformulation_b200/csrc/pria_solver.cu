@@ -58,8 +58,10 @@ constexpr int kXThreads = 256;
 constexpr int kAuxThreads = 256;
 constexpr int kCheckBlock = 256;
 constexpr int kLowTW = 32;              // columns per tile of the lower-bound pass
-constexpr int kSliceBytes = 200 * 1024; // z slice per CTA of a cluster
+constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
 constexpr int kMaxCluster = 16;
+constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
+constexpr int kZUnroll = 4;          // z elements per thread in flight (y/z kernel)
 
 struct Control {
     double omega, theta, fp_error, check_error;
@@ -107,8 +109,11 @@ __device__ __forceinline__ double warp_max(double v) {
 // Michelot's simplex projection threshold for the values v[q], q < len, held
 // by one warp (lane holds q = lane + 32 k): theta with sum max(v - theta, 0) =
 // target.  Fixed point of theta <- (sum_{v > theta} v - target) / #{v > theta}
-// from the all-active start; at most len rounds.  +inf for target <= 0 (the
-// zero simplex).
+// from the all-active start.  In exact arithmetic the active count falls
+// strictly until the fixed point; rounding can move theta back by an ulp and
+// let an element re-enter, which would cycle, so the loop stops as soon as the
+// count does not fall (at most len rounds).  +inf for target <= 0 (the zero
+// simplex).
 template <class Real, int K>
 __device__ double michelot_regs(const Real (&v)[K], int len, double target) {
     if (!(target > 0.0)) return INFINITY;
@@ -133,7 +138,7 @@ __device__ double michelot_regs(const Real (&v)[K], int len, double target) {
         }
         s2 = warp_sum(s2);
         c2 = __reduce_add_sync(0xffffffffu, c2);
-        if (c2 == cnt || c2 == 0) break;
+        if (c2 >= cnt || c2 == 0) break;
         cnt = c2;
         th = (s2 - target) / double(c2);
     }
@@ -162,7 +167,7 @@ __device__ double michelot_smem(const Real* v, int len, double target) {
         }
         s2 = warp_sum(s2);
         c2 = __reduce_add_sync(0xffffffffu, c2);
-        if (c2 == cnt || c2 == 0) break;
+        if (c2 >= cnt || c2 == 0) break;
         cnt = c2;
         th = (s2 - target) / double(c2);
     }
@@ -195,11 +200,27 @@ x_kernel(Dev<Real> d, const Real* xsrc, const Real* __restrict__ ysrc, const Rea
     const int tt = t0 + col;
     const double om = c->omega;
     const Real tau = Real(d.eta / om), sigma = Real(d.eta * om);
-    for (int s = warp * kRpw + sub; s < rows; s += nwarps * kRpw) {
-        if (col < tcols && tt >= s) {
-            const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
-            pre[col * stride + s] = xsrc[e] - tau * ((d.h[e] + ysrc[e]) + zsrc[e]);
+    // rows are taken kUnroll at a time per warp so that their loads are in
+    // flight together
+    const int rstep = nwarps * kRpw;
+    for (int sb = warp * kRpw + sub; sb < rows; sb += rstep * kUnroll) {
+        long long ev[kUnroll];
+        Real xv[kUnroll], hv[kUnroll], yv[kUnroll], zv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int s = sb + u * rstep;
+            ev[u] = -1;
+            if (s < rows && col < tcols && tt >= s) {
+                ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+                xv[u] = xsrc[ev[u]];
+                hv[u] = d.h[ev[u]];
+                yv[u] = ysrc[ev[u]];
+                zv[u] = zsrc[ev[u]];
+            }
         }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (ev[u] >= 0) pre[col * stride + sb + u * rstep] = xv[u] - tau * ((hv[u] + yv[u]) + zv[u]);
     }
     __syncthreads();
     for (int cc = warp; cc < tcols; cc += nwarps) {
@@ -210,12 +231,25 @@ x_kernel(Dev<Real> d, const Real* xsrc, const Real* __restrict__ ysrc, const Rea
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
     double acc[2] = {0.0, 0.0};
-    for (int s = warp * kRpw + sub; s < rows; s += nwarps * kRpw) {
-        if (col < tcols && tt >= s) {
-            const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
-            const Real x2 = Real(fmax(double(pre[col * stride + s]) - theta[col], 0.0));
-            const Real x1 = xsrc[e];
-            const Real xa = Reflect ? d.x0[e] : x1;
+    for (int sb = warp * kRpw + sub; sb < rows; sb += rstep * kUnroll) {
+        long long ev[kUnroll];
+        Real x1v[kUnroll], xav[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int s = sb + u * rstep;
+            ev[u] = -1;
+            if (s < rows && col < tcols && tt >= s) {
+                ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+                x1v[u] = xsrc[ev[u]];
+                xav[u] = Reflect ? d.x0[ev[u]] : x1v[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            if (ev[u] < 0) continue;
+            const long long e = ev[u];
+            const Real x2 = Real(fmax(double(pre[col * stride + sb + u * rstep]) - theta[col], 0.0));
+            const Real x1 = x1v[u], xa = xav[u];
             d.r[e] = sigma * (Real(2) * x2 - x1);
             d.xh[e] = lwn * (Real(2) * x2 - x1) + rwn * xa;
             if (!Reflect) d.x0[e] = x1;
@@ -339,7 +373,7 @@ yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
                 S2 += pp[0];
                 C2 += pp[1];
             }
-            if (C2 == cnt || C2 == 0.0) break;
+            if (C2 >= cnt || C2 == 0.0) break;
             cnt = C2;
             th = (S2 - target) / C2;
         }
@@ -348,19 +382,34 @@ yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
     }
 
     // phase C: z
-    for (int q = threadIdx.x; q < mine; q += kThreads) {
-        const long long e = base + (long long)r0 * len + q;
-        const Real z2 = Real(fmax(double(vz[q]) - thz, 0.0));
-        const Real z1 = zsrc[e];
-        const Real za = Reflect ? d.z0[e] : z1;
-        d.zh[e] = lwn * (Real(2) * z2 - z1) + rwn * za;
-        if (!Reflect) d.z0[e] = z1;
-        if (Check) {
-            if (Reflect) d.z2s[e] = z2;
-            const double dz = double(z1) - double(z2), dr = double(z1) - double(za);
-            acc[0] += dz * dz;
-            acc[1] += double(d.dxs[e]) * dz;
-            acc[2] += dr * dr;
+    const long long sbase = base + (long long)r0 * len;
+    for (int qb = threadIdx.x; qb < mine; qb += kThreads * kZUnroll) {
+        Real z1v[kZUnroll], zav[kZUnroll], dxv[kZUnroll];
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q < mine) {
+                z1v[u] = zsrc[sbase + q];
+                zav[u] = Reflect ? d.z0[sbase + q] : z1v[u];
+                if (Check) dxv[u] = d.dxs[sbase + q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q >= mine) continue;
+            const long long e = sbase + q;
+            const Real z2 = Real(fmax(double(vz[q]) - thz, 0.0));
+            const Real z1 = z1v[u], za = zav[u];
+            d.zh[e] = lwn * (Real(2) * z2 - z1) + rwn * za;
+            if (!Reflect) d.z0[e] = z1;
+            if (Check) {
+                if (Reflect) d.z2s[e] = z2;
+                const double dz = double(z1) - double(z2), dr = double(z1) - double(za);
+                acc[0] += dz * dz;
+                acc[1] += double(dxv[u]) * dz;
+                acc[2] += dr * dr;
+            }
         }
     }
     if (Check) {
@@ -669,7 +718,7 @@ __global__ void __launch_bounds__(kAuxThreads) project_yz_kernel(Dev<Real> d, Re
             __syncthreads();
             const double S2 = bc[0], C2 = bc[1];
             __syncthreads();
-            if (C2 == cnt || C2 == 0.0) break;
+            if (C2 >= cnt || C2 == 0.0) break;
             cnt = C2;
             th = (S2 - target) / C2;
         }
