@@ -93,6 +93,7 @@ struct Dev {
     Real *xh, *x0, *r, *yh, *y0, *zh, *z0;   // combined point (next step), anchors, reflection
     Real *x2s, *dxs, *y2s, *z2s;             // at checks: the step and x1 - x2
     double *px, *pyz, *pup, *plo;            // partial rows
+    double *thx, *thy, *thz;                 // last thresholds: per column, row, block
     Control* ctl;
 };
 
@@ -106,72 +107,94 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// Michelot's simplex projection threshold for the values v[q], q < len, held
-// by one warp (lane holds q = lane + 32 k): theta with sum max(v - theta, 0) =
-// target.  Fixed point of theta <- (sum_{v > theta} v - target) / #{v > theta}
-// from the all-active start.  In exact arithmetic the active count falls
-// strictly until the fixed point; rounding can move theta back by an ulp and
-// let an element re-enter, which would cycle, so the loop stops as soon as the
-// count does not fall (at most len rounds).  +inf for target <= 0 (the zero
-// simplex).
+// Michelot's simplex projection threshold: theta with
+// sum max(v - theta, 0) = target, the fixed point of
+//     theta <- (sum_{v > theta} v - target) / #{v > theta}.
+// From the all-active start the active count falls strictly until the fixed
+// point.  A warm start (the segment's threshold of the previous iteration,
+// which moves little from one iteration to the next) takes the active set at
+// `warm`; the first update from it lands at or below the fixed point whatever
+// side `warm` was on, and from there the count falls again.  When the count
+// stops falling in that monotone phase the loop ends: rounding can move theta
+// back by an ulp and let an element re-enter, which would otherwise cycle.
+// A warm start with an empty active set falls back to the cold start.
+// Returns +inf for target <= 0 (the zero simplex).
+
+// sums over {v > th} for values held by one warp in registers
 template <class Real, int K>
-__device__ double michelot_regs(const Real (&v)[K], int len, double target) {
-    if (!(target > 0.0)) return INFINITY;
+__device__ __forceinline__ void active_regs(const Real (&v)[K], int len, double th, double& S, int& C) {
     const int lane = threadIdx.x & 31;
-    double sum = 0.0;
+    const Real thr = Real(th);
+    Real p = Real(0);
+    int c = 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k)
-        if (lane + 32 * k < len) sum += double(v[k]);
-    sum = warp_sum(sum);
-    double th = (sum - target) / double(len);
-    int cnt = len;
-    for (int round = 0; round < len; ++round) {
-        double s2 = 0.0;
-        int c2 = 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const double x = double(v[k]);
-            if (lane + 32 * k < len && x > th) {
-                s2 += x;
-                ++c2;
-            }
+    for (int k = 0; k < K; ++k) {
+        if (lane + 32 * k < len && (th == -INFINITY || v[k] > thr)) {
+            p += v[k];
+            ++c;
         }
-        s2 = warp_sum(s2);
-        c2 = __reduce_add_sync(0xffffffffu, c2);
-        if (c2 >= cnt || c2 == 0) break;
-        cnt = c2;
-        th = (s2 - target) / double(c2);
+    }
+    S = warp_sum(double(p));
+    C = __reduce_add_sync(0xffffffffu, c);
+}
+
+template <class Real>
+__device__ __forceinline__ void active_smem(const Real* v, int len, double th, double& S, int& C) {
+    const int lane = threadIdx.x & 31;
+    double p = 0.0;
+    int c = 0;
+    for (int q = lane; q < len; q += 32) {
+        const double x = double(v[q]);
+        if (th == -INFINITY || x > th) {
+            p += x;
+            ++c;
+        }
+    }
+    S = warp_sum(p);
+    C = __reduce_add_sync(0xffffffffu, c);
+}
+
+// The Michelot iteration over an `active(th, S, C)` sum routine; `warm` is
+// NaN for a cold start.
+template <class F>
+__device__ __forceinline__ double michelot(F active, int len, double target, double warm) {
+    if (!(target > 0.0)) return INFINITY;
+    double S;
+    int C;
+    bool monotone = true;
+    if (isfinite(warm)) {
+        active(warm, S, C);
+        monotone = false;
+    }
+    if (!isfinite(warm) || C == 0) {
+        active(-INFINITY, S, C);   // all active
+        monotone = true;
+    }
+    double th = (S - target) / double(C);
+    for (int round = 0; round <= len; ++round) {
+        double S2;
+        int C2;
+        active(th, S2, C2);
+        if (C2 == C || C2 == 0) break;
+        if (monotone && C2 > C) break;
+        monotone = true;
+        S = S2;
+        C = C2;
+        th = (S2 - target) / double(C2);
     }
     return th;
 }
 
-// The same threshold for values in shared memory, v[0..len), one warp.
+template <class Real, int K>
+__device__ double michelot_regs(const Real (&v)[K], int len, double target, double warm) {
+    return michelot([&](double th, double& S, int& C) { active_regs(v, len, th, S, C); }, len, target,
+                    warm);
+}
+
 template <class Real>
-__device__ double michelot_smem(const Real* v, int len, double target) {
-    if (!(target > 0.0)) return INFINITY;
-    const int lane = threadIdx.x & 31;
-    double sum = 0.0;
-    for (int q = lane; q < len; q += 32) sum += double(v[q]);
-    sum = warp_sum(sum);
-    double th = (sum - target) / double(len);
-    int cnt = len;
-    for (int round = 0; round < len; ++round) {
-        double s2 = 0.0;
-        int c2 = 0;
-        for (int q = lane; q < len; q += 32) {
-            const double x = double(v[q]);
-            if (x > th) {
-                s2 += x;
-                ++c2;
-            }
-        }
-        s2 = warp_sum(s2);
-        c2 = __reduce_add_sync(0xffffffffu, c2);
-        if (c2 >= cnt || c2 == 0) break;
-        cnt = c2;
-        th = (s2 - target) / double(c2);
-    }
-    return th;
+__device__ double michelot_smem(const Real* v, int len, double target, double warm) {
+    return michelot([&](double th, double& S, int& C) { active_smem(v, len, th, S, C); }, len, target,
+                    warm);
 }
 
 // x half-step of one PDHG step (solver.py:418-421), with the reflection and
@@ -224,8 +247,12 @@ x_kernel(Dev<Real> d, const Real* xsrc, const Real* __restrict__ ysrc, const Rea
     }
     __syncthreads();
     for (int cc = warp; cc < tcols; cc += nwarps) {
-        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0);
-        if (lane == 0) theta[cc] = th;
+        double* slot = d.thx + (long long)item * d.tp + (t0 + cc);
+        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0, *slot);
+        if (lane == 0) {
+            theta[cc] = th;
+            *slot = th;
+        }
     }
     __syncthreads();
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
@@ -287,7 +314,7 @@ yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
     const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* vz = reinterpret_cast<Real*>(smem_raw);
-    __shared__ double part[2];
+    __shared__ double part[2][2];
     __shared__ double scratch[3 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads / 32;
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
@@ -307,7 +334,9 @@ yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
                 vz[(i - r0) * len + q] = zsrc[e0 + q] + rr;
             }
         }
-        const double th = michelot_regs(v, len, double(d.k[i]));
+        double* slot = d.thy + (long long)s * d.n + i;
+        const double th = michelot_regs(v, len, double(d.k[i]), *slot);
+        if (lane == 0) *slot = th;
 #pragma unroll
         for (int k = 0; k < 32; ++k) {
             const int q = lane + 32 * k;
@@ -330,56 +359,41 @@ yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
     }
     __syncthreads();
 
-    // phase B: the z threshold over the whole block, across the cluster
+    // phase B: the z threshold over the whole block, across the cluster.
+    // Each CTA's (sum, count) over its slice goes to part[parity]; after one
+    // cluster barrier every CTA adds all ranks' partials in rank order, so
+    // every CTA takes the same decisions.  The two parities let a round write
+    // its partials while no CTA can still be reading that buffer.
     const int mine = (r1 - r0) * len;
-    const double target = double(d.k0);
-    double thz = INFINITY;
-    if (target > 0.0) {
-        double a[2] = {0.0, double(mine)};
-        for (int q = threadIdx.x; q < mine; q += kThreads) a[0] += double(vz[q]);
-        block_sums<2>(a, scratch, a);
+    int parity = 0;
+    auto active = [&](double th, double& S, int& C) {
+        double b[2] = {0.0, 0.0};
+        for (int q = threadIdx.x; q < mine; q += kThreads) {
+            const double x = double(vz[q]);
+            if (th == -INFINITY || x > th) {
+                b[0] += x;
+                b[1] += 1.0;
+            }
+        }
+        block_sums<2>(b, scratch, b);
         if (threadIdx.x == 0) {
-            part[0] = a[0];
-            part[1] = double(mine);
+            part[parity][0] = b[0];
+            part[parity][1] = b[1];
         }
         cluster.sync();
-        double S = 0.0, C = 0.0;
+        double s0 = 0.0, c0 = 0.0;
         for (int rk = 0; rk < csize; ++rk) {
-            const double* pp = cluster.map_shared_rank(part, rk);
-            S += pp[0];
-            C += pp[1];
+            const double* pp = cluster.map_shared_rank(&part[parity][0], rk);
+            s0 += pp[0];
+            c0 += pp[1];
         }
-        double th = (S - target) / C, cnt = C;
-        const long long total = (long long)d.n * len;
-        for (long long round = 0; round < total; ++round) {
-            cluster.sync();   // every CTA has read `part` before it is rewritten
-            double b[2] = {0.0, 0.0};
-            for (int q = threadIdx.x; q < mine; q += kThreads) {
-                const double x = double(vz[q]);
-                if (x > th) {
-                    b[0] += x;
-                    b[1] += 1.0;
-                }
-            }
-            block_sums<2>(b, scratch, b);
-            if (threadIdx.x == 0) {
-                part[0] = b[0];
-                part[1] = b[1];
-            }
-            cluster.sync();
-            double S2 = 0.0, C2 = 0.0;
-            for (int rk = 0; rk < csize; ++rk) {
-                const double* pp = cluster.map_shared_rank(part, rk);
-                S2 += pp[0];
-                C2 += pp[1];
-            }
-            if (C2 >= cnt || C2 == 0.0) break;
-            cnt = C2;
-            th = (S2 - target) / C2;
-        }
-        thz = th;
-        cluster.sync();   // no CTA leaves while another may still read its `part`
-    }
+        S = s0;
+        C = int(c0);
+        parity ^= 1;
+    };
+    const double thz = michelot(active, d.n * len, double(d.k0), d.thz[s]);
+    cluster.sync();   // no CTA leaves while another may still read its partials
+    if (rank == 0 && threadIdx.x == 0) d.thz[s] = thz;
 
     // phase C: z
     const long long sbase = base + (long long)r0 * len;
@@ -658,7 +672,7 @@ __global__ void __launch_bounds__(kXThreads) project_x_kernel(Dev<Real> d, Real*
         if (col < tcols && tt >= s) pre[col * stride + s] = x[blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s)];
     __syncthreads();
     for (int cc = warp; cc < tcols; cc += nwarps) {
-        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0);
+        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0, NAN);
         if (lane == 0) theta[cc] = th;
     }
     __syncthreads();
@@ -683,7 +697,7 @@ __global__ void __launch_bounds__(kAuxThreads) project_yz_kernel(Dev<Real> d, Re
 #pragma unroll
         for (int k = 0; k < 32; ++k)
             if (lane + 32 * k < len) v[k] = y[e0 + lane + 32 * k];
-        const double th = michelot_regs(v, len, double(d.k[i]));
+        const double th = michelot_regs(v, len, double(d.k[i]), NAN);
 #pragma unroll
         for (int k = 0; k < 32; ++k)
             if (lane + 32 * k < len) y[e0 + lane + 32 * k] = Real(fmax(double(v[k]) - th, 0.0));
@@ -812,7 +826,7 @@ struct Solver final : SolverBase {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     PoolBuf<Real> h, k, xh, x0, r, yh, y0, zh, z0, x2s, dxs, y2s, z2s;
-    PoolBuf<double> px, pyz, pup, plo, final_up;
+    PoolBuf<double> px, pyz, pup, plo, final_up, thx, thy, thz;
     PoolBuf<double> warm[3];   // dense warm start (FP64), optional
     bool has_warm = false;
     PoolBuf<Control> ctl;
@@ -825,7 +839,7 @@ struct Solver final : SolverBase {
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
-    static constexpr int kYZThreads = 512;
+    static constexpr int kYZThreads = 256;
 
     ~Solver() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -834,7 +848,7 @@ struct Solver final : SolverBase {
         for (auto& ev : done) if (ev) cudaEventDestroy(ev);
         for (auto& ev : evpool) cudaEventDestroy(ev);
         for (auto* b : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s}) b->release();
-        for (auto* b : {&px, &pyz, &pup, &plo, &final_up}) b->release();
+        for (auto* b : {&px, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
         for (auto& b : warm) b.release();
         ctl.release();
         if (stream) cudaStreamSynchronize(stream);
@@ -903,6 +917,9 @@ struct Solver final : SolverBase {
         RB_CUDA_TRY(pup.alloc(size_t(tp) * 3, stream));
         RB_CUDA_TRY(plo.alloc(size_t(nblo), stream));
         RB_CUDA_TRY(final_up.alloc(size_t(tp) * 3, stream));
+        RB_CUDA_TRY(thx.alloc(size_t(n) * tp, stream));
+        RB_CUDA_TRY(thy.alloc(size_t(n) * tp, stream));
+        RB_CUDA_TRY(thz.alloc(size_t(tp), stream));
         RB_CUDA_TRY(ctl.alloc(1, stream));
         for (auto& ev : done) RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         d.ntc = ntc;
@@ -913,6 +930,7 @@ struct Solver final : SolverBase {
         d.xh = xh.ptr; d.x0 = x0.ptr; d.r = r.ptr; d.yh = yh.ptr; d.y0 = y0.ptr; d.zh = zh.ptr; d.z0 = z0.ptr;
         d.x2s = x2s.ptr; d.dxs = dxs.ptr; d.y2s = y2s.ptr; d.z2s = z2s.ptr;
         d.px = px.ptr; d.pyz = pyz.ptr; d.pup = pup.ptr; d.plo = plo.ptr; d.ctl = ctl.ptr;
+        d.thx = thx.ptr; d.thy = thy.ptr; d.thz = thz.ptr;
         prm.tolerance = p.tolerance;
         prm.eta = p.eta;
         prm.max_iter = p.max_iter;
@@ -1063,6 +1081,10 @@ struct Solver final : SolverBase {
 
     cudaError_t start_solve() {
         nlaunch = 0;
+        // every run starts its thresholds cold (all-NaN bytes)
+        RB_CUDA_TRY(cudaMemsetAsync(thx.ptr, 0xFF, sizeof(double) * thx.count, stream));
+        RB_CUDA_TRY(cudaMemsetAsync(thy.ptr, 0xFF, sizeof(double) * thy.count, stream));
+        RB_CUDA_TRY(cudaMemsetAsync(thz.ptr, 0xFF, sizeof(double) * thz.count, stream));
         init_kernel<Real><<<tp, 256, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
         nlaunch += 1;
         if (has_warm) {
