@@ -1,0 +1,107 @@
+/* reform.h -- batched and serving forms of the PRAQ / PRIA solvers.
+ *
+ * No counterpart in the reference: it solves one instance per call
+ * (praq_solve) or fans independent solves out over host threads
+ * (pria_solve_batch_*, jrp/pria-cuda/src/pria.cu:15-44).  Here many instances
+ * of uneven size -- QUBO and JRP mixed -- share one engine: every kernel
+ * launch covers all active instances through device-resident work tables
+ * (persistent CTAs and, for the JRP y/z half-step, persistent clusters), each
+ * instance keeps its own restart and termination state on the device, one
+ * op_steps block of all instances replays as one captured CUDA graph, and
+ * finished instances retire between replays by leaving the work tables (no
+ * re-capture).  Instances join between blocks, so a serving loop can admit
+ * requests while others are running.
+ *
+ * Every instance computes exactly what its solo solve computes (same kernels,
+ * same per-instance layout and order of sums), so results are bitwise those of
+ * reform_praq_* / reform_pria_* with the same precision.
+ *
+ * Precision: iterates in FP32 (use_float32 = 1) or FP64; reductions, restart
+ * logic and bounds always FP64.  All instances of a batch share op_steps
+ * (the first instance's; default 16); tolerance and max_iter are per instance.
+ */
+#ifndef REFORM_B200_REFORM_H
+#define REFORM_B200_REFORM_H
+
+#include <stdint.h>
+
+#include "praq.h"
+#include "pria.h"
+
+#ifndef REFORM_API
+#define REFORM_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct reform_batch reform_batch;
+
+/* Tunable launch shapes (reform_batch_autotune picks them; zero = default). */
+typedef struct {
+    int praq_half_edges_per_lane;  /* node-kernel lanes per node target: 2, 4 or 8 */
+    int grid_multiplier;           /* persistent CTAs per SM for the step kernels: 2..16 */
+    int reserved[6];
+} reform_shapes;
+
+/* An empty engine on `stream` (cudaStream_t; NULL: a private one). */
+REFORM_API int reform_batch_create(int use_float32, void* stream, reform_batch** out);
+
+/* Add an instance: validated and laid out on the device now; it joins the
+ * block schedule at reform_batch_start.  Returns its id (>= 0) or a negative
+ * error (PRAQ_ERROR_* for QUBO, -(CUDA error) for JRP). */
+REFORM_API int reform_batch_add_qubo(reform_batch* b, const PraqInstance* instance,
+                                     const PraqParameters* parameters);
+REFORM_API int reform_batch_add_jrp(reform_batch* b, int64_t n, int64_t t, const double* order_costs,
+                                    double joint_cost, const double* holding_costs,
+                                    const pria_params* params);
+
+/* Cold-start every instance added since the last call (the first vanilla step
+ * and the check before the loop) and put it in the work tables. */
+REFORM_API int reform_batch_start(reform_batch* b);
+
+/* Run blocks until every instance has terminated (or `max_blocks` blocks,
+ * < 0: no cap), retiring instances between replays.  Returns 0 or an error. */
+REFORM_API int reform_batch_run(reform_batch* b, int64_t max_blocks);
+
+/* Serving: enqueue one block (a graph replay) without waiting ... */
+REFORM_API int reform_batch_launch(reform_batch* b);
+/* ... and wait for the oldest enqueued block, retire what it finished, and
+ * write up to `max` newly finished ids to `ids` (*count of them).  Returns
+ * the number of instances still running, or a negative error. */
+REFORM_API int reform_batch_sync(reform_batch* b, int* ids, int max, int* count);
+
+/* Number of blocks enqueued and not yet synced. */
+REFORM_API int reform_batch_inflight(const reform_batch* b);
+
+/* Status of instance `id`: done (1 once terminated), iterations, bounds. */
+REFORM_API int reform_batch_status(reform_batch* b, int id, int* done, int64_t* iterations,
+                                   double* lower, double* upper);
+
+/* Results (any output may be NULL): QUBO primal [n]; JRP dense [n][t][t]. */
+REFORM_API int reform_batch_result_qubo(reform_batch* b, int id, double* x, PraqResult* result);
+REFORM_API int reform_batch_result_jrp(reform_batch* b, int id, double* x, double* y, double* z,
+                                       pria_result_info* info);
+
+/* Free an instance's device memory (it must be done or never started). */
+REFORM_API int reform_batch_remove(reform_batch* b, int id);
+
+/* Device bytes held by the instances of the batch (their layouts and iterates). */
+REFORM_API int64_t reform_batch_device_bytes(const reform_batch* b);
+
+/* Launch shapes: set explicitly, or let the autotuner time each candidate on
+ * the batch's own instances (one block each, state restarted afterwards) and
+ * keep the fastest; `out` receives the choice. */
+REFORM_API int reform_batch_set_shapes(reform_batch* b, const reform_shapes* shapes);
+REFORM_API int reform_batch_autotune(reform_batch* b, reform_shapes* out);
+
+/* Kernel launches issued by the engine since creation (graph nodes counted). */
+REFORM_API int64_t reform_batch_launches(const reform_batch* b);
+
+REFORM_API void reform_batch_destroy(reform_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REFORM_B200_REFORM_H */

@@ -55,6 +55,11 @@ class PriaResultInfo(ctypes.Structure):
                 ("dual_objective", c_double), ("relative_gap", c_double)]
 
 
+class ReformShapes(ctypes.Structure):
+    _fields_ = [("praq_half_edges_per_lane", c_int), ("grid_multiplier", c_int),
+                ("reserved", c_int * 6)]
+
+
 _lib = None
 
 
@@ -96,6 +101,26 @@ def _declare(lib):
         "reform_pria_run_profiled": (I, [c_void_p, D, P(c_int64)]),
         "reform_pria_launches": (c_int64, [c_void_p]),
         "reform_pria_destroy": (None, [c_void_p]),
+    })
+    V = c_void_p
+    sig.update({
+        "reform_batch_create": (I, [I, V, P(V)]),
+        "reform_batch_add_qubo": (I, [V, P(PraqInstance), P(PraqParameters)]),
+        "reform_batch_add_jrp": (I, [V, c_int64, c_int64, D, c_double, D, P(PriaParams)]),
+        "reform_batch_start": (I, [V]),
+        "reform_batch_run": (I, [V, c_int64]),
+        "reform_batch_launch": (I, [V]),
+        "reform_batch_sync": (I, [V, P(c_int), I, P(c_int)]),
+        "reform_batch_inflight": (I, [V]),
+        "reform_batch_status": (I, [V, I, P(c_int), P(c_int64), D, D]),
+        "reform_batch_result_qubo": (I, [V, I, D, P(PraqResult)]),
+        "reform_batch_result_jrp": (I, [V, I, D, D, D, P(PriaResultInfo)]),
+        "reform_batch_remove": (I, [V, I]),
+        "reform_batch_device_bytes": (c_int64, [V]),
+        "reform_batch_set_shapes": (I, [V, P(ReformShapes)]),
+        "reform_batch_autotune": (I, [V, P(ReformShapes)]),
+        "reform_batch_launches": (c_int64, [V]),
+        "reform_batch_destroy": (None, [V]),
     })
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

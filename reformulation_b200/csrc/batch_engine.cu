@@ -1,0 +1,942 @@
+// batch_engine.cu -- many PRAQ and PRIA instances of uneven size in one engine
+// (include/reform.h).
+//
+// Each instance keeps the device layout and iterates of its solo solver
+// (praq_core.cuh, pria_core.cuh); this file is a second driver over them.  Per
+// kernel kind there is ONE launch covering every active instance: the work is
+// listed in device-resident tables of (instance, tile) pairs, and a persistent
+// grid (a fixed number of CTAs per SM, or of clusters for the JRP y/z
+// half-step, grouped by cluster size) walks the table.  Each tile runs the
+// same tile function as the solo kernel, with the instance's descriptor
+// copied into shared memory, so every instance computes bitwise what its solo
+// solve computes.  Per-instance restart and termination state stays on the
+// device (each instance's control block); one op_steps block of all
+// instances -- steps, bounds, checks, the gated restart steps, a gather of
+// all control blocks into one host copy -- is one captured CUDA graph.
+// Between replays the host retires finished instances by rewriting the tables
+// and their counts (device memory the graph reads), so the graph is replayed
+// unchanged; instances can also join between replays.
+#include "../../include/reform.h"
+#include "praq_core.cuh"
+#include "pria_core.cuh"
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <tuple>
+#include <vector>
+
+namespace rb200 {
+namespace batch {
+namespace {
+
+struct QMeta {
+    praq::Params prm;
+    int nbn, nbe;
+};
+struct JMeta {
+    pria::Params prm;
+    int nbx, nbyz, nbup, nblo;
+};
+
+// One instance's state as the host needs it after a block.
+struct Summary {
+    double lower, upper, gap;
+    long long iteration;
+    int terminated, restart;
+};
+
+enum Count { kNode = 0, kEdge, kQLow, kX, kUp, kJLow, kQCheck, kJCheck, kYZ0 };
+constexpr int kMaxGroups = 17;   // y/z cluster sizes 1..16
+constexpr int kCounts = kYZ0 + kMaxGroups;
+
+// --- batched kernels: persistent grids over the work tables ---------------
+
+template <class Real, bool Reflect, bool Check>
+__global__ void __launch_bounds__(praq::kBlock)
+bq_node(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
+    __shared__ praq::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        praq::node_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? sd.pred : sd.u2s,
+                                                     Reflect ? sd.predc : sd.u2c, step, 0, gate);
+    }
+}
+
+template <class Real, bool Reflect, bool Check>
+__global__ void __launch_bounds__(praq::kBlock)
+bq_edge(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
+    __shared__ praq::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        praq::edge_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? nullptr : sd.u2s, step, 0, gate);
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(praq::kBlock)
+bq_lower(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count) {
+    __shared__ praq::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        praq::lower_kernel_tile<Real>(sd, w.y, sd.u2s, sd.u2c);
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(praq::kCheckBlock)
+bq_check(const praq::Dev<Real>* devs, const QMeta* metas, const int* __restrict__ list, const int* count,
+         int mode) {
+    const int total = *count;
+    for (int k = blockIdx.x; k < total; k += gridDim.x) {
+        const int id = list[k];
+        const praq::Dev<Real>& d = devs[id];
+        const QMeta& m = metas[id];
+        praq::check_body(d.ctl, m.prm, d.scale, d.pnode, m.nbn, d.pedge, m.nbe, d.plower, m.nbn, mode);
+        __syncthreads();
+    }
+}
+
+template <class Real, int TW, bool Reflect, bool Check>
+__global__ void __launch_bounds__(pria::kXThreads)
+bj_x(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
+    __shared__ pria::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        if (Reflect)
+            pria::x_kernel_tile<Real, TW, Reflect, Check>(sd, w.y, sd.xh, sd.yh, sd.zh, step, gate);
+        else
+            pria::x_kernel_tile<Real, TW, Reflect, Check>(sd, w.y, sd.x2s, sd.y2s, sd.z2s, step, gate);
+    }
+}
+
+// Persistent clusters: cluster c takes tasks c, c + clusters, ...; every CTA
+// of a cluster takes the same task (the y/z half-step of one period block).
+template <class Real, int kThreads, bool Reflect, bool Check>
+__global__ void __launch_bounds__(kThreads)
+bj_yz(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count, int csize, int step,
+      int gate) {
+    __shared__ pria::Dev<Real> sd;
+    const int total = *count;
+    const int nclusters = int(gridDim.x) / csize;
+    for (int t = int(blockIdx.x) / csize; t < total; t += nclusters) {
+        const int2 w = tasks[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        if (Reflect)
+            pria::yz_task<Real, kThreads, Reflect, Check>(sd, w.y, sd.yh, sd.zh, step, gate);
+        else
+            pria::yz_task<Real, kThreads, Reflect, Check>(sd, w.y, sd.y2s, sd.z2s, step, gate);
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(pria::kAuxThreads)
+bj_upper(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count) {
+    __shared__ pria::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tasks[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        pria::upper_kernel_tile<Real>(sd, w.y, sd.x2s, sd.tp, 0);
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(pria::kAuxThreads)
+bj_lower(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count) {
+    __shared__ pria::Dev<Real> sd;
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        pria::lower_kernel_tile<Real>(sd, w.y, sd.y2s, sd.z2s);
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(pria::kCheckBlock)
+bj_check(const pria::Dev<Real>* devs, const JMeta* metas, const int* __restrict__ list, const int* count,
+         int mode) {
+    const int total = *count;
+    for (int k = blockIdx.x; k < total; k += gridDim.x) {
+        const int id = list[k];
+        const pria::Dev<Real>& d = devs[id];
+        const JMeta& m = metas[id];
+        pria::check_body(d.ctl, m.prm, d.px, m.nbx, d.pyz, m.nbyz, d.pup, m.nbup, d.plo, m.nblo, mode);
+        __syncthreads();
+    }
+}
+
+// Every instance's control block into one array (slot = instance slot).
+template <class Real>
+__global__ void b_gather(const praq::Dev<Real>* qdevs, int nq, const pria::Dev<Real>* jdevs, int nj,
+                         const unsigned char* __restrict__ live, Summary* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nq + nj || !live[k]) return;
+    Summary s;
+    if (k < nq) {
+        const praq::Control* c = qdevs[k].ctl;
+        s = Summary{c->lower, c->upper, c->gap, c->iteration, c->terminated, c->restart};
+    } else {
+        const pria::Control* c = jdevs[k - nq].ctl;
+        s = Summary{c->lower, c->upper, c->gap, c->iteration, c->terminated, c->restart};
+    }
+    out[k] = s;
+}
+
+template <class T>
+struct Table {
+    PoolBuf<T> buf;
+    std::vector<T> host;
+    size_t capacity = 0;
+};
+
+struct Shapes {
+    double praq_per_lane = 4.0;
+    int grid_mult = 8;
+};
+
+std::mutex tuned_mu;
+std::map<std::tuple<int, int, int, int, int>, Shapes> tuned;   // size class -> shapes
+
+struct EngineBase {
+    virtual ~EngineBase() = default;
+    virtual int add_qubo(const PraqInstance& in, const PraqParameters& p) = 0;
+    virtual int add_jrp(int64_t n, int64_t t, const double* k, double k0, const double* h,
+                        const pria_params& p) = 0;
+    virtual int start() = 0;
+    virtual int run(int64_t max_blocks) = 0;
+    virtual int launch() = 0;
+    virtual int sync(int* ids, int max, int* count) = 0;
+    virtual int inflight() const = 0;
+    virtual int status(int id, int* done, int64_t* it, double* lo, double* up) = 0;
+    virtual int result_qubo(int id, double* x, PraqResult* r) = 0;
+    virtual int result_jrp(int id, double* x, double* y, double* z, pria_result_info* info) = 0;
+    virtual int remove(int id) = 0;
+    virtual int64_t device_bytes() const = 0;
+    virtual int set_shapes(const reform_shapes& s) = 0;
+    virtual int autotune(reform_shapes* out) = 0;
+    virtual int64_t launches() const = 0;
+};
+
+template <class Real>
+struct Engine final : EngineBase {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sms = 148;
+    int op_steps = 0;
+    Shapes shapes;
+    bool shapes_fixed = false;
+
+    struct QInst {
+        std::unique_ptr<praq::Solver<Real>> s;
+        bool started = false, done = false, live = true;
+        Summary last{};
+    };
+    struct JInst {
+        std::unique_ptr<pria::Solver<Real>> s;
+        bool started = false, done = false, live = true;
+        Summary last{};
+    };
+    std::vector<QInst> q;
+    std::vector<JInst> j;
+    std::vector<std::pair<int, int>> ids;   // id -> (0 QUBO / 1 JRP, index)
+
+    // device copies of descriptors and meta (indexed by instance slot)
+    Table<praq::Dev<Real>> qdevs;
+    Table<QMeta> qmeta;
+    Table<pria::Dev<Real>> jdevs;
+    Table<JMeta> jmeta;
+    Table<int2> t_node, t_edge, t_qlow, t_x, t_up, t_jlow;
+    Table<int2> t_yz[kMaxGroups];
+    Table<int> l_qcheck, l_jcheck;
+    Table<unsigned char> live;
+    PoolBuf<int> counts;
+    PoolBuf<Summary> summary;
+    Summary* hsummary = nullptr;
+    size_t hsummary_cap = 0;
+    int hcounts[kCounts] = {};
+
+    size_t x_smem = 0, yz_smem[kMaxGroups] = {};
+    bool groups[kMaxGroups] = {};
+    int tw = sizeof(Real) == 4 ? 32 : 16;
+    bool dirty = true;          // the graph must be captured again
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> events;
+    int head = 0, pending = 0;   // ring of enqueued blocks
+    long long nlaunch = 0, block_nodes = 0;
+
+    ~Engine() override {
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto ev : events) cudaEventDestroy(ev);
+        q.clear();
+        j.clear();
+        if (hsummary) cudaFreeHost(hsummary);
+        if (stream) cudaStreamSynchronize(stream);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    int init(cudaStream_t s) {
+        if (s) {
+            stream = s;
+        } else {
+            if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) return -int(cudaErrorUnknown);
+            own_stream = true;
+        }
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (counts.alloc(kCounts, stream)) return -int(cudaErrorMemoryAllocation);
+        events.resize(4);
+        for (auto& ev : events)
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) return -int(cudaErrorUnknown);
+        return 0;
+    }
+
+    int add_qubo(const PraqInstance& in, const PraqParameters& p0) override {
+        PraqParameters p = p0;
+        if (!praq::valid(p)) return PRAQ_ERROR_ARGUMENT;
+        if (p.max_iter <= 0) p.max_iter = -1;
+        if (op_steps == 0) op_steps = int(p.op_steps > 0 ? std::max<int64_t>(p.op_steps, 2) : 16);
+        p.op_steps = op_steps;
+        auto s = std::make_unique<praq::Solver<Real>>();
+        s->p = p;
+        const int st = s->setup(in, stream);
+        if (st) return st;
+        s->set_lanes_target(shapes.praq_per_lane);
+        q.push_back(QInst{std::move(s)});
+        ids.emplace_back(0, int(q.size()) - 1);
+        dirty = true;
+        return int(ids.size()) - 1;
+    }
+
+    int add_jrp(int64_t n, int64_t t, const double* k, double k0, const double* h,
+                const pria_params& p0) override {
+        pria_params p = p0;
+        if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
+        p.op_steps = op_steps;
+        std::unique_ptr<pria::SolverBase> base;
+        const int st = pria::create<double>(n, t, k, k0, h, &p, sizeof(Real) == 4, stream, base);
+        if (st) return -st;
+        std::unique_ptr<pria::Solver<Real>> s(static_cast<pria::Solver<Real>*>(base.release()));
+        j.push_back(JInst{std::move(s)});
+        ids.emplace_back(1, int(j.size()) - 1);
+        dirty = true;
+        return int(ids.size()) - 1;
+    }
+
+    template <class T>
+    int upload(Table<T>& tb) {
+        if (tb.host.size() > tb.capacity) {
+            tb.capacity = std::max<size_t>(tb.host.size() * 2, 64);
+            if (tb.buf.alloc(tb.capacity, stream)) return -int(cudaErrorMemoryAllocation);
+            dirty = true;
+        }
+        if (!tb.host.empty() &&
+            cudaMemcpyAsync(tb.buf.ptr, tb.host.data(), sizeof(T) * tb.host.size(), cudaMemcpyHostToDevice,
+                            stream))
+            return -int(cudaErrorUnknown);
+        return 0;
+    }
+
+    // The work tables of the instances that are started and not done,
+    // heaviest tiles first within each kind.
+    int rebuild() {
+        qdevs.host.clear();
+        qmeta.host.clear();
+        for (auto& qi : q) {
+            qdevs.host.push_back(qi.s ? qi.s->d : praq::Dev<Real>{});
+            QMeta m{};
+            if (qi.s) m = QMeta{qi.s->prm, qi.s->nb_node, qi.s->nb_edge};
+            qmeta.host.push_back(m);
+        }
+        jdevs.host.clear();
+        jmeta.host.clear();
+        for (auto& ji : j) {
+            jdevs.host.push_back(ji.s ? ji.s->d : pria::Dev<Real>{});
+            JMeta m{};
+            if (ji.s) m = JMeta{ji.s->prm, ji.s->nbx, ji.s->nbyz, ji.s->tp, ji.s->nblo};
+            jmeta.host.push_back(m);
+        }
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow}) tb->host.clear();
+        for (auto& tb : t_yz) tb.host.clear();
+        l_qcheck.host.clear();
+        l_jcheck.host.clear();
+        live.host.assign(q.size() + j.size(), 0);
+        size_t xs = 0, ys[kMaxGroups] = {};
+        bool gr[kMaxGroups] = {};
+        for (int k = 0; k < int(q.size()); ++k) {
+            auto& qi = q[k];
+            if (!qi.s || !qi.started || qi.done) continue;
+            live.host[k] = 1;
+            for (int t = 0; t < qi.s->nb_node; ++t) {
+                t_node.host.push_back(make_int2(k, t));
+                t_qlow.host.push_back(make_int2(k, t));
+            }
+            if (qi.s->m)
+                for (int t = 0; t < qi.s->nb_edge; ++t) t_edge.host.push_back(make_int2(k, t));
+            l_qcheck.host.push_back(k);
+        }
+        // JRP: x tiles sorted by rows (cost), y/z tasks by block size
+        std::vector<std::pair<long long, int2>> xt, yzt[kMaxGroups], upt;
+        for (int k = 0; k < int(j.size()); ++k) {
+            auto& ji = j[k];
+            if (!ji.s || !ji.started || ji.done) continue;
+            live.host[q.size() + k] = 1;
+            auto& s = *ji.s;
+            const int n = s.n, tp = s.tp, ntc = s.d.ntc;
+            for (int t = 0; t < n * ntc; ++t) {
+                const int ctile = ntc - 1 - t / n;
+                xt.emplace_back((long long)std::min(tp, (ctile + 1) * s.tw), make_int2(k, t));
+            }
+            const int c = s.d.csize;
+            gr[c] = true;
+            ys[c] = std::max(ys[c], s.yz_smem);
+            for (int sb = 0; sb < tp; ++sb) {
+                yzt[c].emplace_back((long long)n * (tp - sb), make_int2(k, sb));
+                upt.emplace_back((long long)n * (tp - sb), make_int2(k, sb));
+            }
+            for (int t = 0; t < s.nblo; ++t) t_jlow.host.push_back(make_int2(k, t));
+            xs = std::max(xs, s.x_smem);
+            l_jcheck.host.push_back(k);
+        }
+        auto order = [](std::vector<std::pair<long long, int2>>& v, Table<int2>& out) {
+            std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            for (auto& e : v) out.host.push_back(e.second);
+        };
+        order(xt, t_x);
+        order(upt, t_up);
+        for (int c = 1; c < kMaxGroups; ++c) order(yzt[c], t_yz[c]);
+        for (int c = 1; c < kMaxGroups; ++c) {
+            if (gr[c] && (!groups[c] || ys[c] > yz_smem[c])) dirty = true;
+            if (gr[c]) {
+                groups[c] = true;
+                yz_smem[c] = std::max(yz_smem[c], ys[c]);
+            }
+        }
+        if (xs > x_smem) {
+            x_smem = xs;
+            dirty = true;
+        }
+        int rc = 0;
+        if ((rc = upload(qdevs)) || (rc = upload(qmeta)) || (rc = upload(jdevs)) || (rc = upload(jmeta))) return rc;
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow})
+            if ((rc = upload(*tb))) return rc;
+        for (int c = 1; c < kMaxGroups; ++c)
+            if (groups[c] && (rc = upload(t_yz[c]))) return rc;
+        if ((rc = upload(l_qcheck)) || (rc = upload(l_jcheck)) || (rc = upload(live))) return rc;
+        hcounts[kNode] = int(t_node.host.size());
+        hcounts[kEdge] = int(t_edge.host.size());
+        hcounts[kQLow] = int(t_qlow.host.size());
+        hcounts[kX] = int(t_x.host.size());
+        hcounts[kUp] = int(t_up.host.size());
+        hcounts[kJLow] = int(t_jlow.host.size());
+        hcounts[kQCheck] = int(l_qcheck.host.size());
+        hcounts[kJCheck] = int(l_jcheck.host.size());
+        for (int c = 0; c < kMaxGroups; ++c) hcounts[kYZ0 + c] = int(t_yz[c].host.size());
+        if (cudaMemcpyAsync(counts.ptr, hcounts, sizeof(hcounts), cudaMemcpyHostToDevice, stream))
+            return -int(cudaErrorUnknown);
+        const size_t slots = q.size() + j.size();
+        if (summary.count < slots) {
+            if (summary.alloc(std::max<size_t>(slots * 2, 64), stream)) return -int(cudaErrorMemoryAllocation);
+            dirty = true;
+        }
+        if (hsummary_cap < summary.count) {
+            if (pending && drain()) return -int(cudaErrorUnknown);   // a block may still copy into it
+            if (hsummary) cudaFreeHost(hsummary);
+            hsummary = nullptr;
+            if (cudaMallocHost(reinterpret_cast<void**>(&hsummary), sizeof(Summary) * summary.count))
+                return -int(cudaErrorMemoryAllocation);
+            hsummary_cap = summary.count;
+        }
+        // (host-to-device copies from pageable memory are staged when issued)
+        return 0;
+    }
+
+    template <bool R, bool C>
+    cudaError_t launch_x(int step, int gate) {
+        const int grid = std::max(1, sms * std::max(1, int((228 * 1024) / std::max<size_t>(x_smem + 2048, 1))));
+        if (tw == 32)
+            bj_x<Real, 32, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
+                                                                        counts.ptr + kX, step, gate);
+        else
+            bj_x<Real, 16, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
+                                                                        counts.ptr + kX, step, gate);
+        return cudaGetLastError();
+    }
+
+    template <bool R, bool C>
+    cudaError_t launch_yz(int c, int step, int gate) {
+        constexpr int kT = pria::Solver<Real>::kYZThreads;
+        const int per_sm = std::max(1, int((228 * 1024) / (yz_smem[c] + 4096)));
+        const int nclusters = std::max(1, (sms * std::min(per_sm, 2)) / c);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(nclusters * c));
+        cfg.blockDim = dim3(kT);
+        cfg.dynamicSmemBytes = yz_smem[c];
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(c);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, bj_yz<Real, kT, R, C>, (const pria::Dev<Real>*)jdevs.buf.ptr,
+                                  (const int2*)t_yz[c].buf.ptr, (const int*)(counts.ptr + kYZ0 + c), c, step,
+                                  gate);
+    }
+
+    cudaError_t set_attributes() {
+        auto xa = [&](auto fn) {
+            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem));
+        };
+        if (tw == 32) {
+            RB_CUDA_TRY(xa(bj_x<Real, 32, true, false>));
+            RB_CUDA_TRY(xa(bj_x<Real, 32, true, true>));
+            RB_CUDA_TRY(xa(bj_x<Real, 32, false, true>));
+        } else {
+            RB_CUDA_TRY(xa(bj_x<Real, 16, true, false>));
+            RB_CUDA_TRY(xa(bj_x<Real, 16, true, true>));
+            RB_CUDA_TRY(xa(bj_x<Real, 16, false, true>));
+        }
+        size_t ym = 0;
+        for (int c = 1; c < kMaxGroups; ++c) ym = std::max(ym, yz_smem[c]);
+        constexpr int kT = pria::Solver<Real>::kYZThreads;
+        auto ya = [&](auto fn) -> cudaError_t {
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ym)));
+            return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        };
+        RB_CUDA_TRY(ya(bj_yz<Real, kT, true, false>));
+        RB_CUDA_TRY(ya(bj_yz<Real, kT, true, true>));
+        RB_CUDA_TRY(ya(bj_yz<Real, kT, false, true>));
+        return cudaSuccess;
+    }
+
+    cudaError_t enqueue_block() {
+        const int gq = sms * shapes.grid_mult;
+        const bool hq = !q.empty(), hj = !j.empty();
+        long long nodes = 0;
+        for (int s = 0; s < op_steps; ++s) {
+            const bool last = s + 1 == op_steps;
+            if (hq) {
+                if (last) {
+                    bq_node<Real, true, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
+                    bq_edge<Real, true, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
+                } else {
+                    bq_node<Real, true, false><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
+                    bq_edge<Real, true, false><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
+                }
+                nodes += 2;
+            }
+            if (hj) {
+                RB_CUDA_TRY((last ? launch_x<true, true>(s, 0) : launch_x<true, false>(s, 0)));
+                nodes += 1;
+                for (int c = 1; c < kMaxGroups; ++c) {
+                    if (!groups[c]) continue;
+                    RB_CUDA_TRY((last ? launch_yz<true, true>(c, s, 0) : launch_yz<true, false>(c, s, 0)));
+                    nodes += 1;
+                }
+            }
+        }
+        if (hq) {
+            bq_lower<Real><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_qlow.buf.ptr, counts.ptr + kQLow);
+            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, stream>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
+                                                                     counts.ptr + kQCheck, 1);
+            bq_node<Real, false, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, 0, 1);
+            bq_edge<Real, false, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, 0, 1);
+            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, stream>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
+                                                                     counts.ptr + kQCheck, 2);
+            nodes += 5;
+        }
+        if (hj) {
+            bj_upper<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_up.buf.ptr, counts.ptr + kUp);
+            bj_lower<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_jlow.buf.ptr, counts.ptr + kJLow);
+            bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
+                                                                     counts.ptr + kJCheck, 1);
+            RB_CUDA_TRY((launch_x<false, true>(0, 1)));
+            nodes += 4;
+            for (int c = 1; c < kMaxGroups; ++c) {
+                if (!groups[c]) continue;
+                RB_CUDA_TRY((launch_yz<false, true>(c, 0, 1)));
+                nodes += 1;
+            }
+            bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
+                                                                     counts.ptr + kJCheck, 2);
+            nodes += 1;
+        }
+        const int slots = int(q.size() + j.size());
+        b_gather<Real><<<std::max(1, ceil_div(slots, 128)), 128, 0, stream>>>(
+            qdevs.buf.ptr, int(q.size()), jdevs.buf.ptr, int(j.size()), live.buf.ptr, summary.ptr);
+        nodes += 1;
+        RB_CUDA_TRY(cudaMemcpyAsync(hsummary, summary.ptr, sizeof(Summary) * slots, cudaMemcpyDeviceToHost, stream));
+        block_nodes = nodes;
+        return cudaGetLastError();
+    }
+
+    int capture() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        if (set_attributes()) return -int(cudaErrorUnknown);
+        if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) return -int(cudaErrorUnknown);
+        const cudaError_t st = enqueue_block();
+        const cudaError_t st2 = cudaStreamEndCapture(stream, &graph);
+        if (st || st2) return -int(st ? st : st2);
+        if (cudaGraphInstantiate(&exec, graph, 0)) return -int(cudaErrorUnknown);
+        dirty = false;
+        return 0;
+    }
+
+    int start() override {
+        if (pending && drain()) return -int(cudaErrorUnknown);
+        for (auto& qi : q) {
+            if (!qi.s || qi.started) continue;
+            const int st = qi.s->start_solve();
+            if (st) return st;
+            qi.started = true;
+            nlaunch += qi.s->launches();
+            qi.done = qi.s->mirror->terminated != 0;
+            const auto* c = qi.s->mirror;
+            qi.last = Summary{c->lower, c->upper, c->gap, c->iteration, c->terminated, 0};
+        }
+        for (auto& ji : j) {
+            if (!ji.s || ji.started) continue;
+            const cudaError_t st = ji.s->start_solve();
+            if (st) return -int(st);
+            ji.started = true;
+            nlaunch += ji.s->launches();
+            ji.done = ji.s->mirror->terminated != 0;
+            const auto* c = ji.s->mirror;
+            ji.last = Summary{c->lower, c->upper, c->gap, c->iteration, c->terminated, 0};
+        }
+        return rebuild();
+    }
+
+    int active() const {
+        int a = 0;
+        for (auto& qi : q) a += qi.s && qi.started && !qi.done;
+        for (auto& ji : j) a += ji.s && ji.started && !ji.done;
+        return a;
+    }
+
+    int launch() override {
+        if (dirty) {
+            if (pending && drain()) return -int(cudaErrorUnknown);
+            const int rc = capture();
+            if (rc) return rc;
+        }
+        if (pending >= int(events.size())) return -int(cudaErrorNotReady);
+        if (cudaGraphLaunch(exec, stream)) return -int(cudaErrorUnknown);
+        if (cudaEventRecord(events[(head + pending) % events.size()], stream)) return -int(cudaErrorUnknown);
+        ++pending;
+        nlaunch += block_nodes;
+        return 0;
+    }
+
+    // Wait for every enqueued block (without retiring anything new).
+    int drain() {
+        if (cudaStreamSynchronize(stream)) return -1;
+        head = (head + pending) % int(events.size());
+        pending = 0;
+        return 0;
+    }
+
+    int sync(int* out_ids, int max, int* count) override {
+        if (count) *count = 0;
+        if (pending == 0) return active();
+        if (cudaEventSynchronize(events[head])) return -int(cudaErrorUnknown);
+        head = (head + 1) % int(events.size());
+        --pending;
+        // the host copy holds the state after this block (or a later one)
+        bool changed = false;
+        int nout = 0;
+        for (int id = 0; id < int(ids.size()); ++id) {
+            const auto [kind, k] = ids[id];
+            const int slot = kind == 0 ? k : int(q.size()) + k;
+            bool* done = kind == 0 ? &q[k].done : &j[k].done;
+            const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
+                                           : (j[k].s && j[k].started && !j[k].done);
+            if (!running) continue;
+            const Summary s = hsummary[slot];
+            (kind == 0 ? q[k].last : j[k].last) = s;
+            if (s.terminated) {
+                *done = true;
+                changed = true;
+                if (out_ids && nout < max) out_ids[nout] = id;
+                ++nout;
+            }
+        }
+        if (count) *count = std::min(nout, max);
+        if (changed) {
+            // blocks already enqueued see the flag and skip the retired
+            // instances; the next ones run without their tiles
+            const int rc = rebuild();
+            if (rc) return rc;
+        }
+        return active();
+    }
+
+    int inflight() const override { return pending; }
+
+    int run(int64_t max_blocks) override {
+        int64_t blocks = 0;
+        while (active() > 0 && (max_blocks < 0 || blocks < max_blocks)) {
+            while (pending < 2 && (max_blocks < 0 || blocks + pending < max_blocks)) {
+                const int rc = launch();
+                if (rc) return rc;
+            }
+            const int rc = sync(nullptr, 0, nullptr);
+            if (rc < 0) return rc;
+            ++blocks;
+        }
+        return drain();
+    }
+
+    int status(int id, int* done, int64_t* it, double* lo, double* up) override {
+        if (id < 0 || id >= int(ids.size())) return PRAQ_ERROR_ARGUMENT;
+        const auto [kind, k] = ids[id];
+        const Summary& s = kind == 0 ? q[k].last : j[k].last;
+        if (done) *done = kind == 0 ? q[k].done : j[k].done;
+        if (it) *it = s.iteration;
+        if (lo) *lo = s.lower;
+        if (up) *up = s.upper;
+        return 0;
+    }
+
+    int result_qubo(int id, double* x, PraqResult* r) override {
+        if (id < 0 || id >= int(ids.size()) || ids[id].first != 0) return PRAQ_ERROR_ARGUMENT;
+        auto& qi = q[ids[id].second];
+        if (!qi.s) return PRAQ_ERROR_ARGUMENT;
+        if (pending && drain()) return PRAQ_ERROR_CUDA;
+        if (cudaMemcpyAsync(qi.s->mirror, qi.s->d.ctl, sizeof(praq::Control), cudaMemcpyDeviceToHost, stream) ||
+            cudaStreamSynchronize(stream))
+            return PRAQ_ERROR_CUDA;
+        return qi.s->result(x, nullptr, r);
+    }
+
+    int result_jrp(int id, double* x, double* y, double* z, pria_result_info* info) override {
+        if (id < 0 || id >= int(ids.size()) || ids[id].first != 1) return int(cudaErrorInvalidValue);
+        auto& ji = j[ids[id].second];
+        if (!ji.s) return int(cudaErrorInvalidValue);
+        if (pending && drain()) return int(cudaErrorUnknown);
+        if (cudaMemcpyAsync(ji.s->mirror, ji.s->d.ctl, sizeof(pria::Control), cudaMemcpyDeviceToHost, stream) ||
+            cudaStreamSynchronize(stream))
+            return int(cudaErrorUnknown);
+        return ji.s->result(x, y, z, info);
+    }
+
+    int remove(int id) override {
+        if (id < 0 || id >= int(ids.size())) return PRAQ_ERROR_ARGUMENT;
+        const auto [kind, k] = ids[id];
+        const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
+                                       : (j[k].s && j[k].started && !j[k].done);
+        if (running) return PRAQ_ERROR_ARGUMENT;
+        if (pending && drain()) return PRAQ_ERROR_CUDA;
+        if (kind == 0) q[k].s.reset(); else j[k].s.reset();
+        return 0;
+    }
+
+    int64_t device_bytes() const override {
+        int64_t b = 0;
+        for (auto& qi : q) if (qi.s) b += int64_t(qi.s->device_bytes());
+        for (auto& ji : j) if (ji.s) b += int64_t(ji.s->device_bytes());
+        return b;
+    }
+
+    int apply_shapes(const Shapes& sh) {
+        shapes = sh;
+        for (auto& qi : q)
+            if (qi.s && qi.s->set_lanes_target(sh.praq_per_lane)) return PRAQ_ERROR_CUDA;
+        dirty = true;
+        return 0;
+    }
+
+    int set_shapes(const reform_shapes& s) override {
+        Shapes sh = shapes;
+        if (s.praq_half_edges_per_lane > 0) sh.praq_per_lane = s.praq_half_edges_per_lane;
+        if (s.grid_multiplier > 0) sh.grid_mult = std::min(16, std::max(1, s.grid_multiplier));
+        shapes_fixed = true;
+        if (pending && drain()) return PRAQ_ERROR_CUDA;
+        const int rc = apply_shapes(sh);
+        return rc ? rc : rebuild();
+    }
+
+    // Restart every started instance from its cold start (used by the tuner).
+    int restart_all() {
+        if (pending && drain()) return -1;
+        for (auto& qi : q) if (qi.s) qi.started = qi.done = false;
+        for (auto& ji : j) if (ji.s) ji.started = ji.done = false;
+        return start();
+    }
+
+    std::tuple<int, int, int, int, int> size_class() const {
+        long long m = 0, nd = 0;
+        int nq = 0, nj = 0;
+        for (auto& qi : q) if (qi.s) { m += qi.s->m; ++nq; }
+        for (auto& ji : j) if (ji.s) { nd += ji.s->d.nd; ++nj; }
+        auto lg = [](long long v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
+        return {nq > 0 ? lg(nq) + 1 : 0, lg(m), nj > 0 ? lg(nj) + 1 : 0, lg(nd), int(sizeof(Real))};
+    }
+
+    // Time one block per candidate shape on this batch's own instances and keep
+    // the fastest; remembered per size class for later batches.
+    int autotune(reform_shapes* out) override {
+        const auto key = size_class();
+        {
+            std::lock_guard<std::mutex> lock(tuned_mu);
+            auto it = tuned.find(key);
+            if (it != tuned.end()) {
+                const int rc = apply_shapes(it->second);
+                if (!rc && out) {
+                    out->praq_half_edges_per_lane = int(it->second.praq_per_lane);
+                    out->grid_multiplier = it->second.grid_mult;
+                }
+                return rc ? rc : restart_all();
+            }
+        }
+        std::vector<Shapes> cands;
+        for (double pl : {2.0, 4.0, 8.0})
+            for (int gm : {2, 4, 8, 16}) cands.push_back(Shapes{pl, gm});
+        if (q.empty()) {
+            cands.clear();
+            for (int gm : {2, 4, 8, 16}) cands.push_back(Shapes{4.0, gm});
+        }
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) || cudaEventCreate(&b)) return -1;
+        float best = 1e30f;
+        Shapes pick = shapes;
+        for (auto& c : cands) {
+            if (apply_shapes(c) || restart_all()) return -1;
+            if (dirty && capture()) return -1;
+            // one untimed block (first touch), then one timed
+            if (cudaGraphLaunch(exec, stream) || cudaStreamSynchronize(stream)) return -1;
+            if (cudaEventRecord(a, stream) || cudaGraphLaunch(exec, stream) || cudaEventRecord(b, stream) ||
+                cudaEventSynchronize(b))
+                return -1;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            nlaunch += 2 * block_nodes;
+            if (ms < best) {
+                best = ms;
+                pick = c;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        {
+            std::lock_guard<std::mutex> lock(tuned_mu);
+            tuned[key] = pick;
+        }
+        if (out) {
+            out->praq_half_edges_per_lane = int(pick.praq_per_lane);
+            out->grid_multiplier = pick.grid_mult;
+        }
+        if (apply_shapes(pick)) return -1;
+        return restart_all();
+    }
+
+    int64_t launches() const override { return nlaunch; }
+};
+
+}  // namespace
+}  // namespace batch
+}  // namespace rb200
+
+using namespace rb200;
+
+struct reform_batch {
+    std::unique_ptr<batch::EngineBase> impl;
+};
+
+extern "C" {
+
+int reform_batch_create(int use_float32, void* stream, reform_batch** out) {
+    if (!out) return PRAQ_ERROR_ARGUMENT;
+    *out = nullptr;
+    auto b = std::make_unique<reform_batch>();
+    int rc;
+    if (use_float32) {
+        auto* e = new batch::Engine<float>();
+        b->impl.reset(e);
+        rc = e->init(static_cast<cudaStream_t>(stream));
+    } else {
+        auto* e = new batch::Engine<double>();
+        b->impl.reset(e);
+        rc = e->init(static_cast<cudaStream_t>(stream));
+    }
+    if (rc) return rc;
+    *out = b.release();
+    return 0;
+}
+
+int reform_batch_add_qubo(reform_batch* b, const PraqInstance* instance, const PraqParameters* parameters) {
+    if (!b || !instance || !parameters) return PRAQ_ERROR_ARGUMENT;
+    const int64_t limit = std::numeric_limits<int>::max();
+    if (instance->n <= 0 || instance->n > limit / 32 || instance->m < 0 || instance->m > limit / 2)
+        return PRAQ_ERROR_INSTANCE;
+    if (!instance->diag || (instance->m > 0 && (!instance->rows || !instance->cols || !instance->vals)))
+        return PRAQ_ERROR_INSTANCE;
+    return b->impl->add_qubo(*instance, *parameters);
+}
+
+int reform_batch_add_jrp(reform_batch* b, int64_t n, int64_t t, const double* k, double k0, const double* h,
+                         const pria_params* params) {
+    if (!b || !params) return -int(cudaErrorInvalidValue);
+    return b->impl->add_jrp(n, t, k, k0, h, *params);
+}
+
+int reform_batch_start(reform_batch* b) { return b ? b->impl->start() : PRAQ_ERROR_ARGUMENT; }
+int reform_batch_run(reform_batch* b, int64_t max_blocks) { return b ? b->impl->run(max_blocks) : PRAQ_ERROR_ARGUMENT; }
+int reform_batch_launch(reform_batch* b) { return b ? b->impl->launch() : PRAQ_ERROR_ARGUMENT; }
+int reform_batch_sync(reform_batch* b, int* ids, int max, int* count) {
+    return b ? b->impl->sync(ids, max, count) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_inflight(const reform_batch* b) { return b ? b->impl->inflight() : 0; }
+int reform_batch_status(reform_batch* b, int id, int* done, int64_t* iterations, double* lower, double* upper) {
+    return b ? b->impl->status(id, done, iterations, lower, upper) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_result_qubo(reform_batch* b, int id, double* x, PraqResult* result) {
+    return b ? b->impl->result_qubo(id, x, result) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_result_jrp(reform_batch* b, int id, double* x, double* y, double* z, pria_result_info* info) {
+    return b ? b->impl->result_jrp(id, x, y, z, info) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_remove(reform_batch* b, int id) { return b ? b->impl->remove(id) : PRAQ_ERROR_ARGUMENT; }
+int64_t reform_batch_device_bytes(const reform_batch* b) { return b ? b->impl->device_bytes() : 0; }
+int reform_batch_set_shapes(reform_batch* b, const reform_shapes* s) {
+    return b && s ? b->impl->set_shapes(*s) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_autotune(reform_batch* b, reform_shapes* out) { return b ? b->impl->autotune(out) : PRAQ_ERROR_ARGUMENT; }
+int64_t reform_batch_launches(const reform_batch* b) { return b ? b->impl->launches() : 0; }
+void reform_batch_destroy(reform_batch* b) { delete b; }
+
+}  // extern "C"

@@ -1,878 +1,6 @@
-// praq_solver.cu -- PRAQ (QUBO roof-dual LP) on B200: restarted, reflected
-// Halpern PDHG on the half-edge lift, FP64 or FP32 iterates with FP64
-// reductions, restart logic and bounds.
-//
-// The algorithm is the reference's (qubo/praq-jax/praq/solver.py, the
-// specification; qubo/praq-cuda/src/solver.cuh, its CUDA port).  The device
-// design is this file's own:
-//
-// * ONE REAL PER EDGE for the dual.  Each edge's dual set is a segment of a
-//   line: covering edges (W_ij > 0) live on {(mu, mu) : -w <= mu <= 0},
-//   packing edges on {(a, w - a) : 0 <= a <= w} (projection.py:16-42).  The
-//   Halpern combination is affine with weights summing to one, so every
-//   iterate (projected or combined) stays on that line, and the pair is
-//   carried as one coordinate u (mu, or a).  The projection of
-//   y + eta omega (q - S r) then collapses to
-//       covering:  mu' = clip(mu + (eta omega / 2)(1 - r_i - r_j), -w, 0)
-//       packing:   a'  = clip(a  + (eta omega / 2)(r_j - r_i),      0, w)
-// * BOTH HALF-EDGE VALUES CONTIGUOUS FOR THE SCATTER.  Edges are sorted by
-//   first end (stable), so a node's first-end half-edges are one run of
-//   `pred` (slot 0 = u).  The edge kernel also writes each edge's slot-1 value
-//   (u, or w - u) into `predc` at the edge's position in second-end order, a
-//   scattered write that costs the writer no stall; the node kernel then reads
-//   its second-end half-edges as one run of `predc`.  The node kernel has no
-//   index indirection at all; the one random read left per edge is the edge
-//   kernel's read of r at both ends (an n-sized array).
-// * `pred`/`predc` hold the NEXT step's Halpern-combined dual, computed by the
-//   edge kernel as it finishes a step (as the reference does), so a reflected
-//   step streams one real per edge of dual state plus the anchor.
-// * Every decision of _halpern_step (restart tests, omega/theta update,
-//   termination) runs on the device in `check_kernel`; one op_steps block
-//   (op_steps x (node, edge), lower-bound pass, check, the gated restart step)
-//   needs no host input, so repeated runs replay it as a captured CUDA graph.
-//   The host keeps one block in flight ahead of the one it inspects.
-// * The instance is laid out ON THE DEVICE from the caller's COO arrays:
-//   validation, scaling, the stable sorts by first and second end (CUB radix
-//   sort; the first is skipped when the input is already sorted by first end),
-//   the run pointers and degrees are kernels, so a one-shot solve pays one
-//   upload of the raw arrays and no O(m) host work.
-//
-// Determinism: every sum has a fixed order that depends on the instance and
-// the launch shape only, so runs are bitwise reproducible.
-#include "../../include/praq.h"
-#include "common.cuh"
-#include "memory.cuh"
-
-#include <cub/device/device_radix_sort.cuh>
-
-#include <algorithm>
-#include <chrono>
-#include <cstring>
-#include <memory>
-
-namespace rb200 {
-namespace praq {
-
-constexpr double kEta = 0.999;   // 0.999 / ||A||_2, ||A||_2 = 1 for the half-edge lift
-constexpr int kBlock = 256;
-constexpr int kEdgesPerThread = 4;
-constexpr int kNodeSums = 3;     // sum deg (x1-x2)^2, sum deg (x1-x0)^2, sum d . bx
-constexpr int kEdgeSums = 5;     // sum |y1-y2|^2, <S(x1-x2), y1-y2>, sum |y1-y0|^2,
-                                 // upper edge term at bx, sum of covering by_1
-constexpr int kCheckBlock = 256;
-constexpr int kPrepBlocks = 296; // fixed grid of the preprocessing reduction
-
-// Scalar state of the solve (StepArguments' scalars, solver.py:229-256),
-// resident on the device.
-struct Control {
-    double omega, theta, fp_error, check_error;
-    double new_error, lower, upper, gap;
-    long long restart_iter, iteration;
-    int terminated;   // the loop is over
-    int restart;      // the restart step of this block is pending
-    int result_slot;  // 1: (x1, u0) hold the returned point, 2: (x2, u2s)
-    int status;
-};
-static_assert(sizeof(Control) <= 256, "a pinned mirror slot holds one Control");
-
-struct Params {
-    double tolerance;
-    long long max_iter, op_steps;
-    double beta_sufficient, beta_necessary, beta_artificial;
-    double theta_target, theta_decay;
-};
-
-template <class Real>
-struct Dev {
-    int n, m, lanes, lane_shift;
-    const int* row_ptr;    // [n+1] first-end runs in sorted edge order
-    const int* col_ptr;    // [n+1] second-end runs in second-end order
-    const int* colpos;     // [m] position of sorted edge s in second-end order
-    const int2* ends;      // [m]
-    const Real* w;         // [m] signed, 2 W_ij / scale
-    const Real* diag;      // [n] W_ii / scale
-    const Real* deg;       // [n] incident half-edges, floored at 1
-    const double* scale;   // [1] objective scale
-    Real *x1, *x2, *x0, *r;
-    Real *pred, *predc;    // next combined dual: slot 0 (sorted order), slot 1 (second-end order)
-    Real *u0;              // anchor (sorted order)
-    Real *u2s, *u2c;       // y2 at the last check, in the two orders
-    double *pnode, *pedge, *plower;
-    Control* ctl;
-};
-
-__device__ __forceinline__ bool skip(const Control* c, int gate) {
-    return c->terminated || (gate && !c->restart);
-}
-
-// S^T y at node i, summed over a group of `lanes` lanes (every lane ends with
-// the same bits): the run [row_ptr[i], row_ptr[i+1]) of `ys` plus the run
-// [col_ptr[i], col_ptr[i+1]) of `yc`.  All lanes of the warp must call it.
-template <class Real, class Acc>
-__device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __restrict__ ys,
-                                          const Real* __restrict__ yc, long long i, int lane) {
-    Acc s0 = Acc(0), s1 = Acc(0);
-    if (i < d.n) {
-        const int L = d.lanes;
-        const int a = d.row_ptr[i], b = d.row_ptr[i + 1];
-        const int c = d.col_ptr[i], e = d.col_ptr[i + 1];
-        int k = a + lane, q = c + lane;
-        // both runs together, unrolled by two: four loads in flight
-        for (; k + L < b && q + L < e; k += 2 * L, q += 2 * L) {
-            const Real v0 = ys[k], v1 = ys[k + L], w0 = yc[q], w1 = yc[q + L];
-            s0 += Acc(v0) + Acc(v1);
-            s1 += Acc(w0) + Acc(w1);
-        }
-        for (; k < b; k += L) s0 += Acc(ys[k]);
-        for (; q < e; q += L) s1 += Acc(yc[q]);
-    }
-    Acc s = s0 + s1;
-    for (int o = d.lanes >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-// Primal half of one PDHG step, with the Halpern combination of x folded in
-// (solver.py:259-267 and 276-292).  Reflect: x1 = lw (2 x2 - x1) + rw x0 with
-// k = restart_iter + step + 1; vanilla: x1 = x2 and the anchor becomes x1.
-// Check: the node sums of this step go to pnode.
-template <class Real, bool Reflect, bool Check>
-__global__ void __launch_bounds__(kBlock)
-node_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
-            int bounds_at_1, int gate) {
-    const Control* c = d.ctl;
-    if (skip(c, gate)) return;
-    __shared__ double scratch[kNodeSums * 32];
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & (d.lanes - 1);
-    const long long i = g >> d.lane_shift;
-    const bool owner = i < d.n && lane == 0;
-    // node data first, so its latency hides behind the gather
-    Real x1o = Real(0), x2o = Real(0), x0o = Real(0), di = Real(0), dg = Real(1);
-    if (owner) {
-        x2o = d.x2[i];
-        di = d.diag[i];
-        dg = d.deg[i];
-        if (Reflect) {
-            x1o = d.x1[i];
-            x0o = d.x0[i];
-        }
-    }
-    const Real s = scatter_at<Real, Real>(d, ys, yc, i, lane);
-    double acc[kNodeSums] = {0.0, 0.0, 0.0};
-    if (owner) {
-        Real x1v;
-        if (Reflect) {
-            const double k = double(c->restart_iter + step + 1);
-            const Real lw = Real(k / (k + 1.0)), rw = Real(1.0 / (k + 1.0));
-            x1v = lw * (Real(2) * x2o - x1o) + rw * x0o;
-        } else {
-            x1v = x2o;
-        }
-        const Real ps = Real(kEta / c->omega);
-        const Real x2v = clampv(x1v - ps * ((di - s) / dg), Real(0), Real(1));
-        d.x1[i] = x1v;
-        d.x2[i] = x2v;
-        d.r[i] = Real(2) * x2v - x1v;
-        if (!Reflect) d.x0[i] = x1v;
-        if (Check) {
-            const double dx = double(x1v) - double(x2v);
-            const double dr = Reflect ? double(x1v) - double(x0o) : 0.0;
-            acc[0] = double(dg) * dx * dx;
-            acc[1] = double(dg) * dr * dr;
-            acc[2] = double(di) * double(bounds_at_1 ? x1v : x2v);
-        }
-    }
-    if (Check) {
-        block_sums<kNodeSums>(acc, scratch, acc);
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < kNodeSums; ++k) d.pnode[size_t(blockIdx.x) * kNodeSums + k] = acc[k];
-        }
-    }
-}
-
-// Dual half of one PDHG step (solver.py:269-273, projection.py:16-42) in the
-// one-coordinate form, plus the prediction of the next step's combined dual.
-// Each thread takes kEdgesPerThread edges a block-stride apart, so all their
-// loads are in flight together.
-template <class Real, bool Reflect, bool Check>
-__global__ void __launch_bounds__(kBlock)
-edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) {
-    const Control* c = d.ctl;
-    if (skip(c, gate)) return;
-    __shared__ double scratch[kEdgeSums * 32];
-    const int base = blockIdx.x * (kBlock * kEdgesPerThread) + threadIdx.x;
-    const Real hs = Real(0.5 * kEta * c->omega);
-    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
-    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
-    int2 ij[kEdgesPerThread];
-    Real sw[kEdgesPerThread], u1[kEdgesPerThread], u0[kEdgesPerThread];
-    int cp[kEdgesPerThread];
-#pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
-        const int e = base + t * kBlock;
-        if (e < d.m) {
-            ij[t] = d.ends[e];
-            sw[t] = d.w[e];
-            u1[t] = Reflect ? d.pred[e] : ysrc[e];
-            u0[t] = Reflect ? d.u0[e] : u1[t];
-            cp[t] = d.colpos[e];
-        }
-    }
-    Real ri[kEdgesPerThread], rj[kEdgesPerThread];
-#pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
-        if (base + t * kBlock < d.m) {
-            ri[t] = d.r[ij[t].x];
-            rj[t] = d.r[ij[t].y];
-        }
-    }
-    double acc[kEdgeSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
-        const int e = base + t * kBlock;
-        if (e >= d.m) continue;
-        const bool cov = sw[t] > Real(0);
-        const Real w = cov ? sw[t] : -sw[t];
-        const Real u2 = cov ? clampv(u1[t] + hs * ((Real(1) - ri[t]) - rj[t]), -w, Real(0))
-                            : clampv(u1[t] + hs * (rj[t] - ri[t]), Real(0), w);
-        const Real nx = lwn * (Real(2) * u2 - u1[t]) + rwn * u0[t];
-        d.pred[e] = nx;
-        d.predc[cp[t]] = cov ? nx : w - nx;
-        if (!Reflect) d.u0[e] = u1[t];
-        if (Check) {
-            if (Reflect) {
-                d.u2s[e] = u2;
-                d.u2c[cp[t]] = cov ? u2 : w - u2;
-            }
-            const double x1i = d.x1[ij[t].x], x2i = d.x2[ij[t].x];
-            const double x1j = d.x1[ij[t].y], x2j = d.x2[ij[t].y];
-            const double dy = double(u1[t]) - double(u2);
-            const double dxi = x1i - x2i, dxj = x1j - x2j;
-            acc[0] += 2.0 * dy * dy;
-            acc[1] += (cov ? dxi + dxj : dxi - dxj) * dy;
-            const double dr = double(u1[t]) - double(u0[t]);
-            acc[2] += 2.0 * dr * dr;
-            const double bi = bounds_at_1 ? x1i : x2i, bj = bounds_at_1 ? x1j : x2j;
-            const double wd = double(w);
-            acc[3] += cov ? wd * fmax(bi + bj - 1.0, 0.0) : -wd * fmin(bi, bj);
-            acc[4] += cov ? double(bounds_at_1 ? u1[t] : u2) : 0.0;
-        }
-    }
-    if (Check) {
-        block_sums<kEdgeSums>(acc, scratch, acc);
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < kEdgeSums; ++k) d.pedge[size_t(blockIdx.x) * kEdgeSums + k] = acc[k];
-        }
-    }
-}
-
-// The node part of the lower bound, sum_i min(d_i - (S^T y)_i, 0), at the
-// dual (ys, yc) (solver.py:333-337), in FP64.
-template <class Real>
-__global__ void __launch_bounds__(kBlock)
-lower_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc) {
-    if (d.ctl->terminated) return;
-    __shared__ double scratch[32];
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & (d.lanes - 1);
-    const long long i = g >> d.lane_shift;
-    const double s = scatter_at<Real, double>(d, ys, yc, i, lane);
-    double acc[1] = {0.0};
-    if (i < d.n && lane == 0) {
-        const double rc = double(d.diag[i]) - s;
-        acc[0] = rc < 0.0 ? rc : 0.0;
-    }
-    block_sums<1>(acc, scratch, acc);
-    if (threadIdx.x == 0) d.plower[blockIdx.x] = acc[0];
-}
-
-__device__ __forceinline__ double canonical(const double* node, const double* edge, double omega) {
-    // + cross term (halpern_operator.py:7-35)
-    const double v = (omega / kEta) * node[0] + (1.0 / (kEta * omega)) * edge[0] + 2.0 * edge[1];
-    return sqrt(v > 0.0 ? v : 0.0);
-}
-
-__device__ __forceinline__ bool should_stop(double gap, long long iteration, const Params& p) {
-    const bool within = iteration < p.max_iter || p.max_iter < 0;
-    const bool outside = !(gap <= p.tolerance);   // NaN keeps going
-    return !(within && outside);
-}
-
-// mode 0: the check before the loop (bounds at (x1, y1));
-// mode 1: the check after an op_steps block (solver.py:397-469);
-// mode 2: after the restart step, the new fixed-point error.
-__global__ void __launch_bounds__(kCheckBlock)
-check_kernel(Control* c, Params p, const double* __restrict__ scale_ptr,
-             const double* __restrict__ pnode, int nbn, const double* __restrict__ pedge, int nbe,
-             const double* __restrict__ plower, int nbl, int mode) {
-    if (c->terminated) return;
-    if (mode == 2 && !c->restart) return;
-    __shared__ double scratch[kEdgeSums * 32];
-    __shared__ double node[kNodeSums], edge[kEdgeSums], low[1];
-    reduce_rows<kNodeSums>(pnode, nbn, scratch, node);
-    reduce_rows<kEdgeSums>(pedge, nbe, scratch, edge);
-    if (mode != 2) reduce_rows<1>(plower, nbl, scratch, low);
-    if (threadIdx.x != 0) return;
-    if (mode == 2) {
-        c->fp_error = canonical(node, edge, c->omega);
-        c->check_error = INFINITY;
-        c->restart_iter = 0;
-        c->restart = 0;
-        return;
-    }
-    const double scale = *scale_ptr;
-    const double upper = (node[2] + edge[3]) * scale;
-    const double lower = (low[0] + edge[4]) * scale;
-    const double gap = (upper - lower) / (1.0 + fabs(upper) + fabs(lower));
-    c->upper = upper;
-    c->lower = lower;
-    c->gap = gap;
-    if (mode == 0) {
-        c->fp_error = canonical(node, edge, c->omega);
-        c->new_error = c->fp_error;
-        c->check_error = INFINITY;
-        c->terminated = should_stop(gap, c->iteration, p) ? 1 : 0;
-        c->result_slot = 1;
-        c->restart = 0;
-        return;
-    }
-    c->iteration += p.op_steps;
-    c->restart_iter += p.op_steps;
-    const double new_err = canonical(node, edge, c->omega);
-    c->new_error = new_err;
-    const bool terminated = should_stop(gap, c->iteration, p);
-    const bool sufficient = new_err <= p.beta_sufficient * c->fp_error;
-    const bool necessary = new_err <= p.beta_necessary * c->fp_error && new_err > c->check_error;
-    const bool artificial = double(c->restart_iter) >= p.beta_artificial * double(c->iteration);
-    const bool restart = sufficient || necessary || artificial;
-    if (restart) {
-        const double pn = sqrt(node[1]), dn = sqrt(edge[2]);
-        if (pn > 1e-16 && dn > 1e-16) {
-            const double th = c->theta;
-            c->omega = exp(th * (log(dn) - log(pn)) + (1.0 - th) * log(c->omega));
-            c->theta = p.theta_target + p.theta_decay * (th - p.theta_target);
-        }
-    }
-    if (terminated) {
-        c->terminated = 1;
-        c->result_slot = 2;
-        c->restart = 0;
-    } else if (restart) {
-        c->restart = 1;
-    } else {
-        c->check_error = new_err;
-    }
-}
-
-// Cold start: the centroid, x = 1/2 and y_e = (-W_ij, -W_ij) / scale, which is
-// u = -w / 2 in the one-coordinate form (half_edge.py:87-94).
-template <class Real>
-__global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta) {
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < d.n) {
-        d.x1[k] = Real(0.5);
-        d.x2[k] = Real(0.5);
-        d.x0[k] = Real(0.5);
-    }
-    if (k < d.m) {
-        const Real sw = d.w[k];
-        const Real u = Real(-0.5) * sw;
-        const Real v = sw > Real(0) ? u : -sw - u;
-        d.u0[k] = u;
-        d.pred[k] = u;
-        d.u2s[k] = u;
-        d.predc[d.colpos[k]] = v;
-        d.u2c[d.colpos[k]] = v;
-    }
-    if (k == 0) {
-        c->omega = omega;
-        c->theta = theta;
-        c->fp_error = 0.0;
-        c->check_error = INFINITY;
-        c->new_error = 0.0;
-        c->lower = c->upper = c->gap = NAN;
-        c->restart_iter = 0;
-        c->iteration = 0;
-        c->terminated = 0;
-        c->restart = 0;
-        c->result_slot = 1;
-        c->status = 0;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// device preprocessing (the reference does this on the host:
-// qubo/praq-cuda/src/solver.cuh:517-569 and qubo/praq-cuda/src/praq.cu:35-79)
-
-// Per edge: range and self-loop check (bit 0 of *flags), first-end order check
-// (bit 1 when some first end is smaller than its predecessor's), int32 keys,
-// and the squares of the objective vector (fixed grid, fixed order).
-__global__ void prep_scan_kernel(long long n, long long m, const int64_t* __restrict__ rows,
-                                 const int64_t* __restrict__ cols, const double* __restrict__ vals,
-                                 const double* __restrict__ diag, int* __restrict__ krow,
-                                 int* __restrict__ kcol, int* flags, double* __restrict__ partial) {
-    __shared__ double scratch[32];
-    double sq = 0.0;
-    int bad = 0, unsorted = 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
-        const int64_t i = rows[e], j = cols[e];
-        if (i < 0 || i >= n || j < 0 || j >= n || i == j) bad = 1;
-        if (e > 0 && rows[e - 1] > i) unsorted = 1;
-        krow[e] = int(i);
-        kcol[e] = int(j);
-        const double v = vals[e];
-        sq += 4.0 * v * v;
-    }
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const double v = diag[i];
-        sq += v * v;
-    }
-    if (bad) atomicOr(flags, 1);
-    if (unsorted) atomicOr(flags, 2);
-    double acc[1] = {sq};
-    block_sums<1>(acc, scratch, acc);
-    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
-}
-
-__global__ void prep_scale_kernel(const double* __restrict__ partial, int count, double* scale) {
-    __shared__ double scratch[32];
-    __shared__ double total[1];
-    reduce_rows<1>(partial, count, scratch, total);
-    if (threadIdx.x == 0) *scale = total[0] > 0.0 ? sqrt(total[0]) : 1.0;
-}
-
-__global__ void iota_kernel(int m, int* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < m) out[k] = k;
-}
-
-// Sorted edge s takes input edge perm[s] (perm null: identity).
-template <class Real>
-__global__ void prep_edges_kernel(int m, const int* __restrict__ perm, const int* __restrict__ krow,
-                                  const int* __restrict__ kcol, const double* __restrict__ vals,
-                                  const double* __restrict__ scale, int2* __restrict__ ends,
-                                  Real* __restrict__ w, int* __restrict__ first,
-                                  int* __restrict__ second, int* __restrict__ sidx) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= m) return;
-    const int e = perm ? perm[s] : s;
-    const int i = krow[e], j = kcol[e];
-    ends[s] = make_int2(i, j);
-    w[s] = Real(2.0 * vals[e] / *scale);
-    first[s] = i;
-    second[s] = j;
-    sidx[s] = s;
-}
-
-// ptr[v] = the first position p of the sorted `keys` with keys[p] >= v, v <= n.
-__global__ void prep_runs_kernel(int n, int m, const int* __restrict__ keys, int* __restrict__ ptr) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v > n) return;
-    int lo = 0, hi = m;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (keys[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    ptr[v] = lo;
-}
-
-__global__ void prep_colpos_kernel(int m, const int* __restrict__ order, int* __restrict__ colpos) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < m) colpos[order[k]] = k;
-}
-
-template <class Real>
-__global__ void prep_nodes_kernel(int n, const int* __restrict__ row_ptr, const int* __restrict__ col_ptr,
-                                  const double* __restrict__ diag, const double* __restrict__ scale,
-                                  Real* __restrict__ dn, Real* __restrict__ deg) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int incident = (row_ptr[i + 1] - row_ptr[i]) + (col_ptr[i + 1] - col_ptr[i]);
-    deg[i] = Real(incident > 0 ? incident : 1);
-    dn[i] = Real(diag[i] / *scale);
-}
-
-// Lanes per node: the smallest power of two (at most a warp) that leaves each
-// lane about four half-edges of the average degree.
-static int lanes_for(int n, int m) {
-    const double average = 2.0 * double(m) / double(n);
-    int lanes = 1;
-    while (lanes < 32 && double(lanes) * 4.0 < average) lanes *= 2;
-    return lanes;
-}
-
-struct SolverBase {
-    virtual ~SolverBase() = default;
-    virtual int run() = 0;
-    virtual int result(double* x, double* y2, PraqResult* r) = 0;
-    virtual long long launches() const = 0;
-    virtual int run_profiled(double* ms, long long* count) = 0;
-    double time_limit = -1.0;   // seconds of wall clock per run; < 0: none
-};
-
-template <class Real>
-struct Solver final : SolverBase {
-    int n = 0, m = 0;
-    Params prm{};
-    PraqParameters p{};
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    PoolBuf<int> row_ptr, col_ptr, colpos, perm;
-    PoolBuf<int2> ends;
-    PoolBuf<Real> w, diag, deg, x1, x2, x0, r, pred, predc, u0, u2s, u2c;
-    PoolBuf<double> pnode, pedge, plower, scale;
-    PoolBuf<Control> ctl;
-    Control* mirror = nullptr;   // pinned host copy of the control block
-    Dev<Real> d{};
-    int nb_node = 1, nb_edge = 1;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    cudaEvent_t done[2] = {nullptr, nullptr};
-    long long nlaunch = 0, block_nodes = 0;
-    int status_override = -100;
-    int runs = 0;
-
-    ~Solver() override {
-        if (stream) cudaStreamSynchronize(stream);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (auto& ev : done) if (ev) cudaEventDestroy(ev);
-        for (auto& ev : evpool) cudaEventDestroy(ev);
-        row_ptr.release(); col_ptr.release(); colpos.release(); perm.release(); ends.release();
-        w.release(); diag.release(); deg.release();
-        x1.release(); x2.release(); x0.release(); r.release(); pred.release(); predc.release();
-        u0.release(); u2s.release(); u2c.release();
-        pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release();
-        if (stream) cudaStreamSynchronize(stream);
-        pinned_put(mirror);
-        if (own_stream && stream) cudaStreamDestroy(stream);
-    }
-
-    // Lay the instance out on the device.  Returns 0, PRAQ_ERROR_INSTANCE or
-    // PRAQ_ERROR_CUDA.
-    int setup(const PraqInstance& in, cudaStream_t s) {
-        if (s) {
-            stream = s;
-        } else {
-            if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
-                return PRAQ_ERROR_CUDA;
-            own_stream = true;
-        }
-        mirror = static_cast<Control*>(pinned_get());
-        if (!mirror) return PRAQ_ERROR_CUDA;
-        const int st = layout(in);
-        if (st) return st;
-        const int lanes = lanes_for(n, m);
-        nb_node = ceil_div((long long)n * lanes, kBlock);
-        nb_edge = std::max(1, ceil_div(m, kBlock * kEdgesPerThread));
-        for (auto* b : {&x1, &x2, &x0, &r})
-            if (b->alloc(n, stream)) return PRAQ_ERROR_CUDA;
-        for (auto* b : {&pred, &predc, &u0, &u2s, &u2c})
-            if (b->alloc(m, stream)) return PRAQ_ERROR_CUDA;
-        if (pnode.alloc(size_t(nb_node) * kNodeSums, stream) ||
-            pedge.alloc(size_t(nb_edge) * kEdgeSums, stream) || plower.alloc(nb_node, stream) ||
-            ctl.alloc(1, stream))
-            return PRAQ_ERROR_CUDA;
-        for (auto& ev : done)
-            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return PRAQ_ERROR_CUDA;
-        d.n = n; d.m = m; d.lanes = lanes;
-        d.lane_shift = 0;
-        while ((1 << d.lane_shift) < lanes) ++d.lane_shift;
-        d.row_ptr = row_ptr.ptr; d.col_ptr = col_ptr.ptr; d.colpos = colpos.ptr;
-        d.ends = ends.ptr; d.w = w.ptr; d.diag = diag.ptr; d.deg = deg.ptr; d.scale = scale.ptr;
-        d.x1 = x1.ptr; d.x2 = x2.ptr; d.x0 = x0.ptr; d.r = r.ptr;
-        d.pred = pred.ptr; d.predc = predc.ptr; d.u0 = u0.ptr; d.u2s = u2s.ptr; d.u2c = u2c.ptr;
-        d.pnode = pnode.ptr; d.pedge = pedge.ptr; d.plower = plower.ptr; d.ctl = ctl.ptr;
-        prm.tolerance = p.tolerance;
-        prm.max_iter = p.max_iter;
-        prm.op_steps = p.op_steps;
-        prm.beta_sufficient = p.beta_sufficient;
-        prm.beta_necessary = p.beta_necessary;
-        prm.beta_artificial = p.beta_artificial;
-        prm.theta_target = p.theta_target;
-        prm.theta_decay = p.theta_decay;
-        block_nodes = (m ? 2 : 1) * (long long)p.op_steps + 2 + (m ? 2 : 1) + 1;
-        return cudaGetLastError() == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
-    }
-
-    int layout(const PraqInstance& in) {
-        n = int(in.n);
-        m = int(in.m);
-        PoolBuf<int64_t> rows, cols;
-        PoolBuf<double> vals, dg, part;
-        PoolBuf<int> krow, kcol, first, second, sidx, flags, keys2, order2, iota, ksorted;
-        PoolBuf<unsigned char> temp;
-        if (dg.upload(in.diag, n, stream) || rows.upload(in.rows, m, stream) ||
-            cols.upload(in.cols, m, stream) || vals.upload(in.vals, m, stream) ||
-            krow.alloc(m, stream) || kcol.alloc(m, stream) || flags.alloc(1, stream) ||
-            part.alloc(kPrepBlocks, stream) || scale.alloc(1, stream))
-            return PRAQ_ERROR_CUDA;
-        if (cudaMemsetAsync(flags.ptr, 0, sizeof(int), stream)) return PRAQ_ERROR_CUDA;
-        prep_scan_kernel<<<kPrepBlocks, kBlock, 0, stream>>>(n, m, rows.ptr, cols.ptr, vals.ptr, dg.ptr,
-                                                            krow.ptr, kcol.ptr, flags.ptr, part.ptr);
-        prep_scale_kernel<<<1, kBlock, 0, stream>>>(part.ptr, kPrepBlocks, scale.ptr);
-        int* hflags = reinterpret_cast<int*>(mirror);   // the pinned slot, before it is a mirror
-        *hflags = 0;
-        if (cudaMemcpyAsync(hflags, flags.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream) ||
-            cudaStreamSynchronize(stream))
-            return PRAQ_ERROR_CUDA;
-        const int fl = *hflags;
-        if (fl & 1) return PRAQ_ERROR_INSTANCE;
-        if (ends.alloc(m, stream) || w.alloc(m, stream) || first.alloc(m, stream) ||
-            second.alloc(m, stream) || sidx.alloc(m, stream) || row_ptr.alloc(n + 1, stream) ||
-            col_ptr.alloc(n + 1, stream) || colpos.alloc(m, stream) || diag.alloc(n, stream) ||
-            deg.alloc(n, stream) || keys2.alloc(m, stream) || order2.alloc(m, stream))
-            return PRAQ_ERROR_CUDA;
-        int key_bits = 1;
-        while (key_bits < 31 && (1LL << key_bits) < (long long)n) ++key_bits;
-        auto radix = [&](const int* kin, int* kout, const int* vin, int* vout) -> int {
-            size_t bytes = 0;
-            if (cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, m, 0, key_bits, stream))
-                return PRAQ_ERROR_CUDA;
-            if (temp.count < bytes && temp.alloc(bytes, stream)) return PRAQ_ERROR_CUDA;
-            if (cub::DeviceRadixSort::SortPairs(temp.ptr, bytes, kin, kout, vin, vout, m, 0, key_bits, stream))
-                return PRAQ_ERROR_CUDA;
-            return 0;
-        };
-        const int* permp = nullptr;
-        if ((fl & 2) && m > 0) {
-            // stable sort of the input edges by first end: perm[s] = input edge
-            if (iota.alloc(m, stream) || ksorted.alloc(m, stream) || perm.alloc(m, stream))
-                return PRAQ_ERROR_CUDA;
-            iota_kernel<<<ceil_div(m, kBlock), kBlock, 0, stream>>>(m, iota.ptr);
-            if (radix(krow.ptr, ksorted.ptr, iota.ptr, perm.ptr)) return PRAQ_ERROR_CUDA;
-            permp = perm.ptr;
-        }
-        if (m > 0) {
-            prep_edges_kernel<Real><<<ceil_div(m, kBlock), kBlock, 0, stream>>>(
-                m, permp, krow.ptr, kcol.ptr, vals.ptr, scale.ptr, ends.ptr, w.ptr, first.ptr,
-                second.ptr, sidx.ptr);
-            // second-end order: a stable sort of the sorted edges by second end
-            if (radix(second.ptr, keys2.ptr, sidx.ptr, order2.ptr)) return PRAQ_ERROR_CUDA;
-            prep_colpos_kernel<<<ceil_div(m, kBlock), kBlock, 0, stream>>>(m, order2.ptr, colpos.ptr);
-        }
-        prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, first.ptr, row_ptr.ptr);
-        prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, keys2.ptr, col_ptr.ptr);
-        prep_nodes_kernel<Real><<<ceil_div(n, kBlock), kBlock, 0, stream>>>(n, row_ptr.ptr, col_ptr.ptr, dg.ptr,
-                                                                          scale.ptr, diag.ptr, deg.ptr);
-        return cudaGetLastError() == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
-    }
-
-    // --- profiling: an event pair around every kernel, by kind ------------
-    static constexpr int kKinds = 9;
-    std::vector<cudaEvent_t> evpool;
-    std::vector<std::pair<int, int>> marks;   // (kind, first event index)
-    bool profiling = false;
-
-    cudaError_t mark_begin(int kind) {
-        if (!profiling) return cudaSuccess;
-        const int idx = int(marks.size()) * 2;
-        while (int(evpool.size()) < idx + 2) {
-            cudaEvent_t ev;
-            RB_CUDA_TRY(cudaEventCreate(&ev));
-            evpool.push_back(ev);
-        }
-        marks.emplace_back(kind, idx);
-        return cudaEventRecord(evpool[idx], stream);
-    }
-    cudaError_t mark_end() {
-        if (!profiling) return cudaSuccess;
-        return cudaEventRecord(evpool[marks.back().second + 1], stream);
-    }
-
-#define RB_TIMED(kind, launch)               \
-    do {                                     \
-        RB_CUDA_TRY(mark_begin(kind));       \
-        launch;                              \
-        RB_CUDA_TRY(mark_end());             \
-    } while (0)
-
-    // One op_steps block: op_steps reflected steps (the last with the check
-    // sums), the lower-bound pass, the check, then the restart step (gated on
-    // the device flag), its error, and a copy of the control block to the host.
-    cudaError_t enqueue_block() {
-        const int op = int(p.op_steps);
-        for (int s = 0; s < op; ++s) {
-            if (s + 1 < op) {
-                RB_TIMED(0, (node_kernel<Real, true, false><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, s, 0, 0)));
-                if (m) RB_TIMED(1, (edge_kernel<Real, true, false><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
-            } else {
-                RB_TIMED(2, (node_kernel<Real, true, true><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, s, 0, 0)));
-                if (m) RB_TIMED(3, (edge_kernel<Real, true, true><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
-            }
-        }
-        RB_TIMED(4, (lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, d.u2c)));
-        RB_TIMED(5, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node,
-                                                                d.pedge, nb_edge, d.plower, nb_node, 1)));
-        RB_TIMED(6, (node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, d.u2c, 0, 0, 1)));
-        if (m) RB_TIMED(7, (edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1)));
-        RB_TIMED(8, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node,
-                                                                d.pedge, nb_edge, d.plower, nb_node, 2)));
-        RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
-        return cudaGetLastError();
-    }
-
-    cudaError_t capture_block() {
-        RB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t st = enqueue_block();
-        cudaError_t st2 = cudaStreamEndCapture(stream, &graph);
-        RB_CUDA_TRY(st);
-        RB_CUDA_TRY(st2);
-        return cudaGraphInstantiate(&exec, graph, 0);
-    }
-
-    cudaError_t launch_block() { return exec ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
-
-    // Cold start, the first vanilla step and the check before the loop.
-    int start_solve() {
-        nlaunch = 0;
-        const int count = std::max(n, m);
-        init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
-        // x1, y1 = _raw_step(x0, y0): one vanilla step from the start, with
-        // the sums for the error and the bounds at the start point.
-        node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, 0, 1, 0);
-        lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc);
-        if (m) edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.pred, 0, 1, 0);
-        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node, d.pedge, nb_edge,
-                                                   d.plower, nb_node, 0);
-        if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-            return PRAQ_ERROR_CUDA;
-        nlaunch += 4 + (m ? 1 : 0);
-        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess)
-            return PRAQ_ERROR_CUDA;
-        return 0;
-    }
-
-    int run() override {
-        const auto started = std::chrono::steady_clock::now();
-        bool timed_out = false;
-        // the first run launches directly; repeated runs replay a captured block
-        if (runs++ > 0 && !exec && capture_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
-        {
-            const int st = start_solve();
-            if (st) return st;
-        }
-        // Keep one block in flight ahead of the one being inspected; blocks
-        // launched after termination see the flag and return at once.
-        if (!mirror->terminated) {
-            for (int k = 0; k < 2; ++k) {
-                if (launch_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
-                if (cudaEventRecord(done[k], stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                nlaunch += block_nodes;
-            }
-            int k = 0;
-            for (;;) {
-                if (cudaEventSynchronize(done[k]) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                if (mirror->terminated) break;
-                if (time_limit >= 0.0 &&
-                    std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() >
-                        time_limit) {
-                    timed_out = true;
-                    break;
-                }
-                if (launch_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
-                if (cudaEventRecord(done[k], stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                nlaunch += block_nodes;
-                k ^= 1;
-            }
-        }
-        if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess)
-            return PRAQ_ERROR_CUDA;
-        if (timed_out && !mirror->terminated) {
-            mirror->result_slot = 2;
-            status_override = PRAQ_STATUS_TIME_LIMIT;
-            return PRAQ_STATUS_TIME_LIMIT;
-        }
-        status_override = -100;
-        return mirror->gap <= p.tolerance ? 0 : 1;
-    }
-
-    // A solve with every kernel launched on its own (no graph) between an
-    // event pair; each kind's total milliseconds and launch count go to
-    // ms[kKinds], count[kKinds].  Same arithmetic; the host waits after every
-    // block.
-    int run_profiled(double* ms, long long* count) override {
-        for (int k = 0; k < kKinds; ++k) { ms[k] = 0.0; count[k] = 0; }
-        int st = start_solve();
-        if (st) return st;
-        profiling = true;
-        while (!mirror->terminated) {
-            marks.clear();
-            if (enqueue_block() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
-                profiling = false;
-                return PRAQ_ERROR_CUDA;
-            }
-            nlaunch += block_nodes;
-            for (auto& mk : marks) {
-                float t = 0.f;
-                if (cudaEventElapsedTime(&t, evpool[mk.second], evpool[mk.second + 1]) != cudaSuccess) {
-                    profiling = false;
-                    return PRAQ_ERROR_CUDA;
-                }
-                ms[mk.first] += t;
-                count[mk.first] += 1;
-            }
-        }
-        profiling = false;
-        if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess)
-            return PRAQ_ERROR_CUDA;
-        status_override = -100;
-        return mirror->gap <= p.tolerance ? 0 : 1;
-    }
-
-    int result(double* x, double* y2, PraqResult* res) override {
-        const Control c = *mirror;
-        if (x) {
-            std::vector<Real> hx(n);
-            const Real* src = c.result_slot == 1 ? d.x1 : d.x2;
-            if (cudaMemcpyAsync(hx.data(), src, sizeof(Real) * n, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-                cudaStreamSynchronize(stream) != cudaSuccess)
-                return PRAQ_ERROR_CUDA;
-            for (int i = 0; i < n; ++i) x[i] = double(hx[i]);
-        }
-        if (y2 && m) {
-            std::vector<Real> hu(m), hw(m);
-            std::vector<int> hp(perm.ptr ? m : 0);
-            double sc = 1.0;
-            const Real* src = c.result_slot == 1 ? d.u0 : d.u2s;
-            if (cudaMemcpyAsync(hu.data(), src, sizeof(Real) * m, cudaMemcpyDeviceToHost, stream) ||
-                cudaMemcpyAsync(hw.data(), d.w, sizeof(Real) * m, cudaMemcpyDeviceToHost, stream) ||
-                cudaMemcpyAsync(&sc, d.scale, sizeof(double), cudaMemcpyDeviceToHost, stream) ||
-                (perm.ptr && cudaMemcpyAsync(hp.data(), perm.ptr, sizeof(int) * m, cudaMemcpyDeviceToHost, stream)) ||
-                cudaStreamSynchronize(stream))
-                return PRAQ_ERROR_CUDA;
-            for (int s = 0; s < m; ++s) {
-                const int e = perm.ptr ? hp[s] : s;
-                const double u = double(hu[s]), sw = double(hw[s]);
-                y2[2 * e] = u * sc;
-                y2[2 * e + 1] = (sw > 0.0 ? u : (-sw - u)) * sc;
-            }
-        }
-        if (res) {
-            res->lower = c.lower;
-            res->upper = c.upper;
-            res->iterations = c.iteration;
-            res->status = status_override != -100 ? status_override : (c.gap <= p.tolerance ? 0 : 1);
-        }
-        return 0;
-    }
-
-    long long launches() const override { return nlaunch; }
-};
-
-static bool valid(const PraqParameters& p) {
-    return p.tolerance >= 0.0 && p.omega > 0.0 && p.beta_sufficient > 0.0 &&
-           p.beta_necessary > 0.0 && p.beta_artificial >= 0.0 && std::isfinite(p.theta_initial) &&
-           std::isfinite(p.theta_target) && std::isfinite(p.theta_decay) &&
-           std::isfinite(p.interval_offset) && std::isfinite(p.interval_scale) &&
-           p.interval_power >= 0.0;
-}
-
-}  // namespace praq
-}  // namespace rb200
+// praq_solver.cu -- the C ABI of the PRAQ solver (include/praq.h); the
+// solver itself (kernels, device layout, host driver) is praq_core.cuh.
+#include "praq_core.cuh"
 
 using namespace rb200;
 

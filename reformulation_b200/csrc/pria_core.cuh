@@ -1,0 +1,1296 @@
+// pria_core.cuh -- PRIA (the joint replenishment LP) on B200: restarted,
+// reflected Halpern PDHG on upper-triangular simplices, FP64 or FP32 iterates
+// with FP64 reductions, restart logic and bounds.
+//
+// The algorithm is the reference's (jrp/pria-jax/pria/solver.py, the
+// specification; jrp/pria-cuda/src/*.cuh, its CUDA port):
+//     x' = P_X(x - tau (h + y + z))         per (i, t): the column s <= t onto
+//                                           the unit simplex
+//     r  = sigma (2 x' - x)
+//     y' = P_Y(y + r)                       per (i, s): the row t >= s onto the
+//                                           K_i simplex
+//     z' = P_Z(z + r)                       per s: the group {(i, t >= s)} onto
+//                                           the K0 simplex
+// with the Halpern combination, the canonical norm with a NEGATIVE cross term
+// (halpern_operator.py:5-19), the bounds of solver.py:347-402 and the restart
+// logic of solver.py:514-594.
+//
+// Device design (this file's own):
+// * PERIOD-MAJOR PACKED TRIANGLE.  Entry (i, s, t), s <= t < Tp, lives at
+//   blk(s) + i (Tp - s) + (t - s), blk(s) = N (s Tp - s (s - 1) / 2): block s
+//   holds every item's row s.  A y row is contiguous, a z group is one
+//   contiguous block, and an x column is one short run per block.
+// * x HALF-STEP: one CTA per (item, tile of TW columns), heaviest tiles first.
+//   It reads the tile's row runs coalesced (TW consecutive periods per row),
+//   forms pre = x - tau (h + y + z) in a shared-memory tile stored column-major
+//   with an odd column stride (bank-conflict free for the column passes), runs
+//   one warp-level Michelot projection per column (theta <- (sum_{v>theta} v -
+//   1) / #{v > theta} to the fixed point, warp-shuffle sums), and writes the
+//   reflection r and the next step's combined x.
+// * y/z HALF-STEP: one thread-block CLUSTER per period block s.  Each warp
+//   projects y rows held in registers (Michelot, shuffles); the block's z
+//   values sit in the CTAs' shared memory and the z Michelot runs across the
+//   cluster, each round exchanging (sum, count) through distributed shared
+//   memory.  r is read once for both.
+// * x, y, z hold the NEXT step's Halpern-combined point (as PRAQ's dual), so a
+//   reflected step streams x, x0, h, y, z (x kernel) and y, y0, z, z0, r (y/z
+//   kernel) and writes x, r, y, z: 14 ND reals per iteration.
+// * Decisions on the device (check_kernel); a block of op_steps steps plus
+//   the gated restart step replays as a captured CUDA graph.
+#pragma once
+
+#include "../../include/pria.h"
+#include "common.cuh"
+#include "memory.cuh"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <memory>
+
+namespace cg = cooperative_groups;
+
+namespace rb200 {
+namespace pria {
+namespace {
+
+constexpr int kMaxPeriods = 1024;       // padded periods (a y row lives in 32 registers per lane)
+constexpr int kXThreads = 256;
+constexpr int kAuxThreads = 256;
+constexpr int kCheckBlock = 256;
+constexpr int kLowTW = 32;              // columns per tile of the lower-bound pass
+constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
+constexpr int kMaxCluster = 16;
+constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
+constexpr int kZUnroll = 4;          // z elements per thread in flight (y/z kernel)
+
+struct Control {
+    double omega, theta, fp_error, check_error;
+    double new_error, lower, upper, gap;
+    long long restart_iter, iteration;
+    int terminated, restart, result_slot, status;
+};
+
+struct Params {
+    double tolerance, eta;
+    long long max_iter, op_steps;
+    double beta_sufficient, beta_necessary, beta_artificial;
+    double theta_target, theta_decay;
+    double scale;
+};
+
+__host__ __device__ __forceinline__ long long blk(int n, int tp, int s) {
+    return (long long)n * ((long long)s * tp - (long long)s * (s - 1) / 2);
+}
+
+template <class Real>
+struct Dev {
+    int n, t, tp, ntc, ntc_low, csize;
+    long long nd;
+    double eta;
+    const Real* h;           // [nd] holding costs / scale
+    const Real* k;           // [n] K_i / scale
+    Real k0;                 // K0 / scale
+    Real *xh, *x0, *r, *yh, *y0, *zh, *z0;   // combined point (next step), anchors, reflection
+    Real *x2s, *dxs, *y2s, *z2s;             // at checks: the step and x1 - x2
+    double *px, *pyz, *pup, *plo;            // partial rows
+    double *thx, *thy, *thz;                 // last thresholds: per column, row, block
+    Control* ctl;
+};
+
+__device__ __forceinline__ bool skip(const Control* c, int gate) {
+    return c->terminated || (gate && !c->restart);
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Michelot's simplex projection threshold: theta with
+// sum max(v - theta, 0) = target, the fixed point of
+//     theta <- (sum_{v > theta} v - target) / #{v > theta}.
+// From the all-active start the active count falls strictly until the fixed
+// point.  A warm start (the segment's threshold of the previous iteration,
+// which moves little from one iteration to the next) takes the active set at
+// `warm`; the first update from it lands at or below the fixed point whatever
+// side `warm` was on, and from there the count falls again.  When the count
+// stops falling in that monotone phase the loop ends: rounding can move theta
+// back by an ulp and let an element re-enter, which would otherwise cycle.
+// A warm start with an empty active set falls back to the cold start.
+// Returns +inf for target <= 0 (the zero simplex).
+
+// sums over {v > th} for values held by one warp in registers
+template <class Real, int K>
+__device__ __forceinline__ void active_regs(const Real (&v)[K], int len, double th, double& S, int& C) {
+    const int lane = threadIdx.x & 31;
+    const Real thr = Real(th);
+    Real p = Real(0);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (lane + 32 * k < len && (th == -INFINITY || v[k] > thr)) {
+            p += v[k];
+            ++c;
+        }
+    }
+    S = warp_sum(double(p));
+    C = __reduce_add_sync(0xffffffffu, c);
+}
+
+template <class Real>
+__device__ __forceinline__ void active_smem(const Real* v, int len, double th, double& S, int& C) {
+    const int lane = threadIdx.x & 31;
+    double p = 0.0;
+    int c = 0;
+    for (int q = lane; q < len; q += 32) {
+        const double x = double(v[q]);
+        if (th == -INFINITY || x > th) {
+            p += x;
+            ++c;
+        }
+    }
+    S = warp_sum(p);
+    C = __reduce_add_sync(0xffffffffu, c);
+}
+
+// The Michelot iteration over an `active(th, S, C)` sum routine; `warm` is
+// NaN for a cold start.
+template <class F>
+__device__ __forceinline__ double michelot(F active, int len, double target, double warm) {
+    if (!(target > 0.0)) return INFINITY;
+    double S;
+    int C;
+    bool monotone = true;
+    if (isfinite(warm)) {
+        active(warm, S, C);
+        monotone = false;
+    }
+    if (!isfinite(warm) || C == 0) {
+        active(-INFINITY, S, C);   // all active
+        monotone = true;
+    }
+    double th = (S - target) / double(C);
+    for (int round = 0; round <= len; ++round) {
+        double S2;
+        int C2;
+        active(th, S2, C2);
+        if (C2 == C || C2 == 0) break;
+        if (monotone && C2 > C) break;
+        monotone = true;
+        S = S2;
+        C = C2;
+        th = (S2 - target) / double(C2);
+    }
+    return th;
+}
+
+template <class Real, int K>
+__device__ double michelot_regs(const Real (&v)[K], int len, double target, double warm) {
+    return michelot([&](double th, double& S, int& C) { active_regs(v, len, th, S, C); }, len, target,
+                    warm);
+}
+
+template <class Real>
+__device__ double michelot_smem(const Real* v, int len, double target, double warm) {
+    return michelot([&](double th, double& S, int& C) { active_smem(v, len, th, S, C); }, len, target,
+                    warm);
+}
+
+// x half-step of one PDHG step (solver.py:418-421), with the reflection and
+// the next combined x.  Reflect: the point stepped from is xsrc (= xh);
+// vanilla: xsrc is the point itself and becomes the anchor.  Check: x2 and
+// x1 - x2 are kept and the x sums go to px.
+template <class Real, int TW, bool Reflect, bool Check>
+__device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, const Real* xsrc, const Real* __restrict__ ysrc, const Real* __restrict__ zsrc,
+         int step, int gate) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* pre = reinterpret_cast<Real*>(smem_raw);
+    __shared__ double theta[TW];
+    __shared__ double scratch[2 * 32];
+    const int item = tile % d.n;
+    const int ctile = d.ntc - 1 - int(tile / d.n);   // heaviest tiles first
+    const int t0 = ctile * TW;
+    const int tcols = min(TW, d.tp - t0);
+    const int rows = t0 + tcols;
+    const int stride = rows | 1;
+    constexpr int kRpw = 32 / TW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int col = lane % TW, sub = lane / TW;
+    const int tt = t0 + col;
+    const double om = c->omega;
+    const Real tau = Real(d.eta / om), sigma = Real(d.eta * om);
+    // rows are taken kUnroll at a time per warp so that their loads are in
+    // flight together
+    const int rstep = nwarps * kRpw;
+    for (int sb = warp * kRpw + sub; sb < rows; sb += rstep * kUnroll) {
+        long long ev[kUnroll];
+        Real xv[kUnroll], hv[kUnroll], yv[kUnroll], zv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int s = sb + u * rstep;
+            ev[u] = -1;
+            if (s < rows && col < tcols && tt >= s) {
+                ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+                xv[u] = xsrc[ev[u]];
+                hv[u] = d.h[ev[u]];
+                yv[u] = ysrc[ev[u]];
+                zv[u] = zsrc[ev[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (ev[u] >= 0) pre[col * stride + sb + u * rstep] = xv[u] - tau * ((hv[u] + yv[u]) + zv[u]);
+    }
+    __syncthreads();
+    for (int cc = warp; cc < tcols; cc += nwarps) {
+        double* slot = d.thx + (long long)item * d.tp + (t0 + cc);
+        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0, *slot);
+        if (lane == 0) {
+            theta[cc] = th;
+            *slot = th;
+        }
+    }
+    __syncthreads();
+    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
+    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    double acc[2] = {0.0, 0.0};
+    for (int sb = warp * kRpw + sub; sb < rows; sb += rstep * kUnroll) {
+        long long ev[kUnroll];
+        Real x1v[kUnroll], xav[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int s = sb + u * rstep;
+            ev[u] = -1;
+            if (s < rows && col < tcols && tt >= s) {
+                ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+                x1v[u] = xsrc[ev[u]];
+                xav[u] = Reflect ? d.x0[ev[u]] : x1v[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            if (ev[u] < 0) continue;
+            const long long e = ev[u];
+            const Real x2 = Real(fmax(double(pre[col * stride + sb + u * rstep]) - theta[col], 0.0));
+            const Real x1 = x1v[u], xa = xav[u];
+            d.r[e] = sigma * (Real(2) * x2 - x1);
+            d.xh[e] = lwn * (Real(2) * x2 - x1) + rwn * xa;
+            if (!Reflect) d.x0[e] = x1;
+            if (Check) {
+                d.x2s[e] = x2;
+                d.dxs[e] = x1 - x2;
+                const double dx = double(x1) - double(x2), dr = double(x1) - double(xa);
+                acc[0] += dx * dx;
+                acc[1] += dr * dr;
+            }
+        }
+    }
+    if (Check) {
+        block_sums<2>(acc, scratch, acc);
+        if (threadIdx.x == 0) {
+            d.px[size_t(tile) * 2] = acc[0];
+            d.px[size_t(tile) * 2 + 1] = acc[1];
+        }
+    }
+}
+
+template <class Real, int TW, bool Reflect, bool Check>
+__global__ void __launch_bounds__(kXThreads)
+x_kernel(Dev<Real> d, const Real* xsrc, const Real* __restrict__ ysrc, const Real* __restrict__ zsrc,
+         int step, int gate) {
+    x_kernel_tile<Real, TW, Reflect, Check>(d, blockIdx.x, xsrc, ysrc, zsrc, step, gate);
+}
+
+// y and z half-steps (solver.py:421-423) for period block s, one cluster of
+// `csize` CTAs per block; CTA `rank` owns rows [r0, r1) of the block.
+template <class Real, int kThreads, bool Reflect, bool Check>
+__device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* ysrc, const Real* zsrc, int step, int gate) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
+    cg::cluster_group cluster = cg::this_cluster();
+    const int csize = d.csize;
+    const int rank = int(cluster.block_rank());
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* vz = reinterpret_cast<Real*>(smem_raw);
+    __shared__ double part[2][2];
+    __shared__ double scratch[3 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads / 32;
+    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
+    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    double acc[3] = {0.0, 0.0, 0.0};   // |dy|^2 + |dz|^2, <dx, dy + dz>, drift
+
+    // phase A: y rows, and the z values into shared memory
+    for (int i = r0 + warp; i < r1; i += nwarps) {
+        const long long e0 = base + (long long)i * len;
+        Real v[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const int q = lane + 32 * k;
+            if (q < len) {
+                const Real rr = d.r[e0 + q];
+                v[k] = ysrc[e0 + q] + rr;
+                vz[(i - r0) * len + q] = zsrc[e0 + q] + rr;
+            }
+        }
+        double* slot = d.thy + (long long)s * d.n + i;
+        const double th = michelot_regs(v, len, double(d.k[i]), *slot);
+        if (lane == 0) *slot = th;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const int q = lane + 32 * k;
+            if (q < len) {
+                const long long e = e0 + q;
+                const Real y2 = Real(fmax(double(v[k]) - th, 0.0));
+                const Real y1 = ysrc[e];
+                const Real ya = Reflect ? d.y0[e] : y1;
+                d.yh[e] = lwn * (Real(2) * y2 - y1) + rwn * ya;
+                if (!Reflect) d.y0[e] = y1;
+                if (Check) {
+                    if (Reflect) d.y2s[e] = y2;
+                    const double dy = double(y1) - double(y2), dr = double(y1) - double(ya);
+                    acc[0] += dy * dy;
+                    acc[1] += double(d.dxs[e]) * dy;
+                    acc[2] += dr * dr;
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // phase B: the z threshold over the whole block, across the cluster.
+    // Each CTA's (sum, count) over its slice goes to part[parity]; after one
+    // cluster barrier every CTA adds all ranks' partials in rank order, so
+    // every CTA takes the same decisions.  The two parities let a round write
+    // its partials while no CTA can still be reading that buffer.
+    const int mine = (r1 - r0) * len;
+    int parity = 0;
+    auto active = [&](double th, double& S, int& C) {
+        double b[2] = {0.0, 0.0};
+        for (int q = threadIdx.x; q < mine; q += kThreads) {
+            const double x = double(vz[q]);
+            if (th == -INFINITY || x > th) {
+                b[0] += x;
+                b[1] += 1.0;
+            }
+        }
+        block_sums<2>(b, scratch, b);
+        if (threadIdx.x == 0) {
+            part[parity][0] = b[0];
+            part[parity][1] = b[1];
+        }
+        cluster.sync();
+        double s0 = 0.0, c0 = 0.0;
+        for (int rk = 0; rk < csize; ++rk) {
+            const double* pp = cluster.map_shared_rank(&part[parity][0], rk);
+            s0 += pp[0];
+            c0 += pp[1];
+        }
+        S = s0;
+        C = int(c0);
+        parity ^= 1;
+    };
+    const double thz = michelot(active, d.n * len, double(d.k0), d.thz[s]);
+    cluster.sync();   // no CTA leaves while another may still read its partials
+    if (rank == 0 && threadIdx.x == 0) d.thz[s] = thz;
+
+    // phase C: z
+    const long long sbase = base + (long long)r0 * len;
+    for (int qb = threadIdx.x; qb < mine; qb += kThreads * kZUnroll) {
+        Real z1v[kZUnroll], zav[kZUnroll], dxv[kZUnroll];
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q < mine) {
+                z1v[u] = zsrc[sbase + q];
+                zav[u] = Reflect ? d.z0[sbase + q] : z1v[u];
+                if (Check) dxv[u] = d.dxs[sbase + q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q >= mine) continue;
+            const long long e = sbase + q;
+            const Real z2 = Real(fmax(double(vz[q]) - thz, 0.0));
+            const Real z1 = z1v[u], za = zav[u];
+            d.zh[e] = lwn * (Real(2) * z2 - z1) + rwn * za;
+            if (!Reflect) d.z0[e] = z1;
+            if (Check) {
+                if (Reflect) d.z2s[e] = z2;
+                const double dz = double(z1) - double(z2), dr = double(z1) - double(za);
+                acc[0] += dz * dz;
+                acc[1] += double(dxv[u]) * dz;
+                acc[2] += dr * dr;
+            }
+        }
+    }
+    if (Check) {
+        block_sums<3>(acc, scratch, acc);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 3; ++k) d.pyz[(size_t(s) * csize + rank) * 3 + k] = acc[k];
+        }
+    }
+}
+
+template <class Real, int kThreads, bool Reflect, bool Check>
+__global__ void __launch_bounds__(kThreads)
+yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
+    yz_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, ysrc, zsrc, step, gate);
+}
+
+// The primal bound terms at x for period block s (solver.py:347-365):
+// sum_i K_i max_{t>=s} x_ist, K0 max_{i, t>=s} x_ist and sum h x over the
+// block, restricted to t < tlimit and s < tlimit (tlimit = t for the unpadded
+// objective).  `force` runs it after termination.
+template <class Real>
+__device__ __forceinline__ void upper_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ x, int tlimit, int force) {
+    if (!force && d.ctl->terminated) return;
+    __shared__ double scratch[3 * 32];
+    __shared__ double wmax[32];
+    const int s = tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double acc[3] = {0.0, 0.0, 0.0};
+    double bmax = 0.0;
+    if (s < tlimit) {
+        const int len = d.tp - s, valid = tlimit - s;
+        const long long base = blk(d.n, d.tp, s);
+        for (int i = warp; i < d.n; i += nwarps) {
+            const long long e0 = base + (long long)i * len;
+            double mx = 0.0, hx = 0.0;
+            for (int q = lane; q < valid; q += 32) {
+                const double v = double(x[e0 + q]);
+                mx = fmax(mx, v);
+                hx += double(d.h[e0 + q]) * v;
+            }
+            mx = warp_max(mx);
+            hx = warp_sum(hx);
+            if (lane == 0) {
+                acc[0] += double(d.k[i]) * mx;
+                acc[2] += hx;
+                bmax = fmax(bmax, mx);
+            }
+        }
+    }
+    if (lane == 0) wmax[warp] = bmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < nwarps; ++w) b = fmax(b, wmax[w]);
+        acc[1] = double(d.k0) * b;
+    }
+    block_sums<3>(acc, scratch, acc);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 3; ++k) d.pup[size_t(s) * 3 + k] = acc[k];
+    }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kAuxThreads)
+upper_kernel(Dev<Real> d, const Real* __restrict__ x, int tlimit, int force) {
+    upper_kernel_tile<Real>(d, blockIdx.x, x, tlimit, force);
+}
+
+// The dual bound sum_{i,t} min_{s<=t} (h + y + z) (solver.py:388-402) for one
+// tile of kLowTW columns of one item.
+template <class Real>
+__device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ y, const Real* __restrict__ z) {
+    if (d.ctl->terminated) return;
+    __shared__ double cmin[kAuxThreads / 32][kLowTW];
+    __shared__ double scratch[32];
+    const int item = tile % d.n;
+    const int ctile = d.ntc_low - 1 - int(tile / d.n);
+    const int t0 = ctile * kLowTW;
+    const int tcols = min(kLowTW, d.tp - t0);
+    const int rows = t0 + tcols;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int tt = t0 + lane;
+    double mn = INFINITY;
+    for (int s = warp; s < rows; s += nwarps) {
+        if (lane < tcols && tt >= s) {
+            const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+            mn = fmin(mn, (double(d.h[e]) + double(y[e])) + double(z[e]));
+        }
+    }
+    cmin[warp][lane] = mn;
+    __syncthreads();
+    double acc[1] = {0.0};
+    if (warp == 0 && lane < tcols) {
+        double v = INFINITY;
+        for (int w = 0; w < nwarps; ++w) v = fmin(v, cmin[w][lane]);
+        acc[0] = v;
+    }
+    block_sums<1>(acc, scratch, acc);
+    if (threadIdx.x == 0) d.plo[tile] = acc[0];
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kAuxThreads)
+lower_kernel(Dev<Real> d, const Real* __restrict__ y, const Real* __restrict__ z) {
+    lower_kernel_tile<Real>(d, blockIdx.x, y, z);
+}
+
+__device__ __forceinline__ double canonical(const double* xs, const double* yzs, double omega,
+                                            double eta) {
+    const double v = (omega / eta) * xs[0] + (1.0 / (eta * omega)) * yzs[0] - 2.0 * yzs[1];
+    return sqrt(v > 0.0 ? v : 0.0);
+}
+
+__device__ __forceinline__ bool should_stop(double gap, long long iteration, const Params& p) {
+    const bool within = iteration < p.max_iter || p.max_iter < 0;
+    return !(within && !(gap <= p.tolerance));   // NaN keeps going
+}
+
+// mode 0: the check before the loop; 1: after an op_steps block; 2: after the
+// restart step (solver.py:514-594).
+__device__ __forceinline__ void check_body(Control* c, Params p, const double* __restrict__ px, int nbx,
+             const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
+             const double* __restrict__ plo, int nblo, int mode) {
+    if (c->terminated) return;
+    if (mode == 2 && !c->restart) return;
+    __shared__ double scratch[3 * 32];
+    __shared__ double xs[2], yzs[3], up[3], lo[1];
+    reduce_rows<2>(px, nbx, scratch, xs);
+    reduce_rows<3>(pyz, nbyz, scratch, yzs);
+    if (mode != 2) {
+        reduce_rows<3>(pup, nbup, scratch, up);
+        reduce_rows<1>(plo, nblo, scratch, lo);
+    }
+    if (threadIdx.x != 0) return;
+    if (mode == 2) {
+        c->fp_error = canonical(xs, yzs, c->omega, p.eta);
+        c->check_error = INFINITY;
+        c->restart_iter = 0;
+        c->restart = 0;
+        return;
+    }
+    const double upper = (up[0] + up[1] + up[2]) * p.scale;
+    const double lower = lo[0] * p.scale;
+    const double gap = (upper - lower) / (1.0 + fabs(lower) + fabs(upper));
+    c->upper = upper;
+    c->lower = lower;
+    c->gap = gap;
+    if (mode == 0) {
+        c->fp_error = canonical(xs, yzs, c->omega, p.eta);
+        c->new_error = c->fp_error;
+        c->check_error = INFINITY;
+        c->terminated = should_stop(gap, c->iteration, p) ? 1 : 0;
+        c->result_slot = 1;
+        c->restart = 0;
+        return;
+    }
+    c->iteration += p.op_steps;
+    c->restart_iter += p.op_steps;
+    const double new_err = canonical(xs, yzs, c->omega, p.eta);
+    c->new_error = new_err;
+    const bool terminated = should_stop(gap, c->iteration, p);
+    const bool sufficient = new_err <= p.beta_sufficient * c->fp_error;
+    const bool necessary = new_err <= p.beta_necessary * c->fp_error && new_err > c->check_error;
+    const bool artificial = double(c->restart_iter) >= p.beta_artificial * double(c->iteration);
+    const bool restart = sufficient || necessary || artificial;
+    if (restart) {
+        const double pn = sqrt(xs[1]), dn = sqrt(yzs[2]);
+        if (pn > 1e-16 && dn > 1e-16) {
+            const double th = c->theta;
+            c->omega = exp(th * (log(dn) - log(pn)) + (1.0 - th) * log(c->omega));
+            c->theta = p.theta_target + p.theta_decay * (th - p.theta_target);
+        }
+    }
+    if (terminated) {
+        c->terminated = 1;
+        c->result_slot = 2;
+        c->restart = 0;
+    } else if (restart) {
+        c->restart = 1;
+    } else {
+        c->check_error = new_err;
+    }
+}
+
+__global__ void __launch_bounds__(kCheckBlock)
+check_kernel(Control* c, Params p, const double* __restrict__ px, int nbx,
+             const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
+             const double* __restrict__ plo, int nblo, int mode) {
+    check_body(c, p, px, nbx, pyz, nbyz, pup, nbup, plo, nblo, mode);
+}
+
+// The start point: the projection of zero, i.e. each simplex's centre:
+// x = 1/(t+1), y = K_i/(Tp-s), z = K0/(N(Tp-s)) (solver.py:669-671), one CTA
+// per period block.  Also resets the control block.
+template <class Real>
+__global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta) {
+    const int s = blockIdx.x;
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const long long count = (long long)d.n * len;
+    const Real zc = d.k0 > Real(0) ? Real(double(d.k0) / double(count)) : Real(0);
+    for (long long q = threadIdx.x; q < count; q += blockDim.x) {
+        const int i = int(q / len), t = s + int(q % len);
+        const Real kv = d.k[i];
+        d.x0[base + q] = Real(1.0 / double(t + 1));
+        d.y0[base + q] = kv > Real(0) ? Real(double(kv) / double(len)) : Real(0);
+        d.z0[base + q] = zc;
+    }
+    if (s == 0 && threadIdx.x == 0) {
+        c->omega = omega;
+        c->theta = theta;
+        c->fp_error = 0.0;
+        c->check_error = INFINITY;
+        c->new_error = 0.0;
+        c->lower = c->upper = c->gap = NAN;
+        c->restart_iter = 0;
+        c->iteration = 0;
+        c->terminated = 0;
+        c->restart = 0;
+        c->result_slot = 1;
+        c->status = 0;
+    }
+}
+
+// Warm start: dense [n][t][t] (normalised duals) -> the packed layout, duals
+// scaled back onto the K_i / K0 simplices (solver.py:662-671); zero padding.
+template <class Real>
+__global__ void warm_pack_kernel(Dev<Real> d, const double* __restrict__ wx, const double* __restrict__ wy,
+                                 const double* __restrict__ wz, Real* __restrict__ px, Real* __restrict__ py,
+                                 Real* __restrict__ pz) {
+    const int s = blockIdx.x;
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const long long count = (long long)d.n * len;
+    for (long long q = threadIdx.x; q < count; q += blockDim.x) {
+        const int i = int(q / len), t = s + int(q % len);
+        Real vx = Real(0), vy = Real(0), vz = Real(0);
+        if (s < d.t && t < d.t) {
+            const long long g = ((long long)i * d.t + s) * d.t + t;
+            vx = Real(wx[g]);
+            vy = Real(wy[g] * double(d.k[i]));
+            vz = Real(wz[g] * double(d.k0));
+        }
+        px[base + q] = vx;
+        py[base + q] = vy;
+        pz[base + q] = vz;
+    }
+}
+
+// Projections of a packed point onto X, Y, Z (for a warm start): the column,
+// row and block passes of the step kernels with nothing else around them.
+template <class Real, int TW>
+__global__ void __launch_bounds__(kXThreads) project_x_kernel(Dev<Real> d, Real* x) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* pre = reinterpret_cast<Real*>(smem_raw);
+    __shared__ double theta[TW];
+    const int item = blockIdx.x % d.n;
+    const int ctile = d.ntc - 1 - int(blockIdx.x / d.n);
+    const int t0 = ctile * TW;
+    const int tcols = min(TW, d.tp - t0);
+    const int rows = t0 + tcols;
+    const int stride = rows | 1;
+    constexpr int kRpw = 32 / TW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int col = lane % TW, sub = lane / TW;
+    const int tt = t0 + col;
+    for (int s = warp * kRpw + sub; s < rows; s += nwarps * kRpw)
+        if (col < tcols && tt >= s) pre[col * stride + s] = x[blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s)];
+    __syncthreads();
+    for (int cc = warp; cc < tcols; cc += nwarps) {
+        const double th = michelot_smem(pre + cc * stride, t0 + cc + 1, 1.0, NAN);
+        if (lane == 0) theta[cc] = th;
+    }
+    __syncthreads();
+    for (int s = warp * kRpw + sub; s < rows; s += nwarps * kRpw)
+        if (col < tcols && tt >= s)
+            x[blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s)] =
+                Real(fmax(double(pre[col * stride + s]) - theta[col], 0.0));
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kAuxThreads) project_yz_kernel(Dev<Real> d, Real* y, Real* z) {
+    // one CTA per block s: y rows by warps, then z over the whole block
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double scratch[2 * 32];
+    const int s = blockIdx.x;
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int i = warp; i < d.n; i += nwarps) {
+        const long long e0 = base + (long long)i * len;
+        Real v[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            if (lane + 32 * k < len) v[k] = y[e0 + lane + 32 * k];
+        const double th = michelot_regs(v, len, double(d.k[i]), NAN);
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            if (lane + 32 * k < len) y[e0 + lane + 32 * k] = Real(fmax(double(v[k]) - th, 0.0));
+    }
+    // z: the whole block through global memory (a one-off projection)
+    const long long count = (long long)d.n * len;
+    const double target = double(d.k0);
+    double th = INFINITY;
+    if (target > 0.0) {
+        double a[2] = {0.0, 0.0};
+        for (long long q = threadIdx.x; q < count; q += blockDim.x) a[0] += double(z[base + q]);
+        block_sums<2>(a, scratch, a);
+        __shared__ double bc[2];
+        if (threadIdx.x == 0) bc[0] = a[0];
+        __syncthreads();
+        th = (bc[0] - target) / double(count);
+        double cnt = double(count);
+        for (long long round = 0; round < count; ++round) {
+            double b[2] = {0.0, 0.0};
+            for (long long q = threadIdx.x; q < count; q += blockDim.x) {
+                const double x = double(z[base + q]);
+                if (x > th) {
+                    b[0] += x;
+                    b[1] += 1.0;
+                }
+            }
+            block_sums<2>(b, scratch, b);
+            if (threadIdx.x == 0) {
+                bc[0] = b[0];
+                bc[1] = b[1];
+            }
+            __syncthreads();
+            const double S2 = bc[0], C2 = bc[1];
+            __syncthreads();
+            if (C2 >= cnt || C2 == 0.0) break;
+            cnt = C2;
+            th = (S2 - target) / C2;
+        }
+    }
+    for (long long q = threadIdx.x; q < count; q += blockDim.x)
+        z[base + q] = Real(fmax(double(z[base + q]) - th, 0.0));
+    (void)smem_raw;
+}
+
+// Packed -> dense [n][t][t] output, unpadded; y / K_i and z / K0 (zero when
+// the budget is zero), mode 0 x, 1 y, 2 z.
+template <class Real, class Out>
+__global__ void unpack_kernel(Dev<Real> d, const Real* __restrict__ src, int mode, Out* __restrict__ out) {
+    const long long total = (long long)d.n * d.t * d.t;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const int t = int(g % d.t);
+        const int s = int((g / d.t) % d.t);
+        const int i = int(g / ((long long)d.t * d.t));
+        double v = 0.0;
+        if (t >= s) {
+            v = double(src[blk(d.n, d.tp, s) + (long long)i * (d.tp - s) + (t - s)]);
+            if (mode == 1) v = d.k[i] > Real(0) ? v / double(d.k[i]) : 0.0;
+            if (mode == 2) v = d.k0 > Real(0) ? v / double(d.k0) : 0.0;
+        }
+        out[g] = Out(v);
+    }
+}
+
+// Input: dense H -> sum of squares of its upper triangle (fixed grid, fixed
+// order) and the packed, scaled h.
+template <class In>
+__global__ void h_squares_kernel(int n, int t, const In* __restrict__ H, double* __restrict__ partial) {
+    __shared__ double scratch[32];
+    const long long total = (long long)n * t * t;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    double acc[1] = {0.0};
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const int tt = int(g % t), s = int((g / t) % t);
+        if (tt >= s) {
+            const double v = double(H[g]);
+            acc[0] += v * v;
+        }
+    }
+    block_sums<1>(acc, scratch, acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+}
+
+template <class In, class Real>
+__global__ void h_pack_kernel(Dev<Real> d, const In* __restrict__ H, double inv_scale, Real* __restrict__ h) {
+    const int s = blockIdx.x;
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const long long count = (long long)d.n * len;
+    for (long long q = threadIdx.x; q < count; q += blockDim.x) {
+        const int i = int(q / len), t = s + int(q % len);
+        double v = 0.0;
+        if (s < d.t && t < d.t) v = double(H[((long long)i * d.t + s) * d.t + t]) * inv_scale;
+        h[base + q] = Real(v);
+    }
+}
+
+constexpr int kSquareBlocks = 296;
+
+__global__ void sum_rows_kernel(const double* __restrict__ partial, int count, double* out) {
+    __shared__ double scratch[32];
+    __shared__ double total[1];
+    reduce_rows<1>(partial, count, scratch, total);
+    if (threadIdx.x == 0) *out = total[0];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+struct SolverBase {
+    virtual ~SolverBase() = default;
+    virtual int run() = 0;
+    virtual int result(double* x, double* y, double* z, pria_result_info* info) = 0;
+    virtual int result_f32(float* x, float* y, float* z, pria_result_info* info) = 0;
+    virtual int set_warm(const double* wx, const double* wy, const double* wz) = 0;
+    virtual long long launches() const = 0;
+    virtual int run_profiled(double* ms, long long* count) = 0;
+};
+
+template <class Real>
+struct Solver final : SolverBase {
+    int n = 0, t = 0, tp = 0;
+    long long nd = 0;
+    pria_params p{};
+    Params prm{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    PoolBuf<Real> h, k, xh, x0, r, yh, y0, zh, z0, x2s, dxs, y2s, z2s;
+    PoolBuf<double> px, pyz, pup, plo, final_up, thx, thy, thz;
+    PoolBuf<double> warm[3];   // dense warm start (FP64), optional
+    bool has_warm = false;
+    PoolBuf<Control> ctl;
+    Control* mirror = nullptr;
+    Dev<Real> d{};
+    int tw = 32, nbx = 1, nbyz = 1, nblo = 1;
+    size_t x_smem = 0, yz_smem = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    long long nlaunch = 0, block_nodes = 0;
+    int runs = 0;
+    static constexpr int kYZThreads = 256;
+
+    ~Solver() override {
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto& ev : done) if (ev) cudaEventDestroy(ev);
+        for (auto& ev : evpool) cudaEventDestroy(ev);
+        for (auto* b : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s}) b->release();
+        for (auto* b : {&px, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
+        for (auto& b : warm) b.release();
+        ctl.release();
+        if (stream) cudaStreamSynchronize(stream);
+        pinned_put(mirror);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    template <class In>
+    cudaError_t setup(int64_t n_, int64_t t_, const In* K, double K0, const In* H, cudaStream_t s) {
+        n = int(n_);
+        t = int(t_);
+        tp = t + (t & 1);
+        nd = (long long)n * tp * (tp + 1) / 2;
+        if (s) {
+            stream = s;
+        } else {
+            RB_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        }
+        mirror = static_cast<Control*>(pinned_get());
+        if (!mirror) return cudaErrorMemoryAllocation;
+        // scale = ||(triu H, K, K0)||_2 (solver.py:652-654)
+        double hsq = 0.0;
+        {
+            PoolBuf<In> Hd;
+            PoolBuf<double> part, tot;
+            RB_CUDA_TRY(Hd.upload(H, size_t(n) * t * t, stream));
+            RB_CUDA_TRY(part.alloc(kSquareBlocks, stream));
+            RB_CUDA_TRY(tot.alloc(1, stream));
+            h_squares_kernel<In><<<kSquareBlocks, 256, 0, stream>>>(n, t, Hd.ptr, part.ptr);
+            sum_rows_kernel<<<1, 256, 0, stream>>>(part.ptr, kSquareBlocks, tot.ptr);
+            double* hp = reinterpret_cast<double*>(mirror);
+            RB_CUDA_TRY(cudaMemcpyAsync(hp, tot.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream));
+            RB_CUDA_TRY(cudaStreamSynchronize(stream));
+            hsq = *hp;
+            double ss = K0 * K0 + hsq;
+            for (int i = 0; i < n; ++i) ss += double(K[i]) * double(K[i]);
+            prm.scale = ss > 0.0 ? std::sqrt(ss) : 1.0;
+            std::vector<Real> ks(n);
+            for (int i = 0; i < n; ++i) ks[i] = Real(double(K[i]) / prm.scale);
+            RB_CUDA_TRY(k.upload(ks.data(), n, stream));
+            RB_CUDA_TRY(h.alloc(nd, stream));
+            d.n = n; d.t = t; d.tp = tp; d.nd = nd;
+            d.k = k.ptr;
+            d.k0 = Real(K0 / prm.scale);
+            h_pack_kernel<In, Real><<<tp, 256, 0, stream>>>(d, Hd.ptr, 1.0 / prm.scale, h.ptr);
+            RB_CUDA_TRY(cudaGetLastError());
+        }
+        for (auto* b : {&xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s})
+            RB_CUDA_TRY(b->alloc(nd, stream));
+        tw = sizeof(Real) == 4 ? 32 : 16;
+        const int ntc = (tp + tw - 1) / tw;
+        const int ntc_low = (tp + kLowTW - 1) / kLowTW;
+        nbx = n * ntc;
+        nblo = n * ntc_low;
+        x_smem = size_t(tw) * size_t(tp | 1) * sizeof(Real);
+        int csize = 1;
+        while (csize < kMaxCluster && (size_t((n + csize - 1) / csize) * tp * sizeof(Real)) > size_t(kSliceBytes))
+            ++csize;
+        if (csize > n) csize = n;
+        yz_smem = size_t((n + csize - 1) / csize) * tp * sizeof(Real);
+        if (yz_smem > size_t(kSliceBytes)) return cudaErrorInvalidValue;
+        nbyz = tp * csize;
+        RB_CUDA_TRY(px.alloc(size_t(nbx) * 2, stream));
+        RB_CUDA_TRY(pyz.alloc(size_t(nbyz) * 3, stream));
+        RB_CUDA_TRY(pup.alloc(size_t(tp) * 3, stream));
+        RB_CUDA_TRY(plo.alloc(size_t(nblo), stream));
+        RB_CUDA_TRY(final_up.alloc(size_t(tp) * 3, stream));
+        RB_CUDA_TRY(thx.alloc(size_t(n) * tp, stream));
+        RB_CUDA_TRY(thy.alloc(size_t(n) * tp, stream));
+        RB_CUDA_TRY(thz.alloc(size_t(tp), stream));
+        RB_CUDA_TRY(ctl.alloc(1, stream));
+        for (auto& ev : done) RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        d.ntc = ntc;
+        d.ntc_low = ntc_low;
+        d.csize = csize;
+        d.eta = p.eta;
+        d.h = h.ptr;
+        d.xh = xh.ptr; d.x0 = x0.ptr; d.r = r.ptr; d.yh = yh.ptr; d.y0 = y0.ptr; d.zh = zh.ptr; d.z0 = z0.ptr;
+        d.x2s = x2s.ptr; d.dxs = dxs.ptr; d.y2s = y2s.ptr; d.z2s = z2s.ptr;
+        d.px = px.ptr; d.pyz = pyz.ptr; d.pup = pup.ptr; d.plo = plo.ptr; d.ctl = ctl.ptr;
+        d.thx = thx.ptr; d.thy = thy.ptr; d.thz = thz.ptr;
+        prm.tolerance = p.tolerance;
+        prm.eta = p.eta;
+        prm.max_iter = p.max_iter;
+        prm.op_steps = p.op_steps;
+        prm.beta_sufficient = p.beta_sufficient;
+        prm.beta_necessary = p.beta_necessary;
+        prm.beta_artificial = p.beta_artificial;
+        prm.theta_target = p.theta_target;
+        prm.theta_decay = p.theta_decay;
+        RB_CUDA_TRY(set_attributes());
+        block_nodes = 2LL * p.op_steps + 3 + 3;
+        return cudaGetLastError();
+    }
+
+    template <int TW, bool R, bool C>
+    cudaError_t x_attr() {
+        return cudaFuncSetAttribute(x_kernel<Real, TW, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(x_smem));
+    }
+    template <bool R, bool C>
+    cudaError_t yz_attr() {
+        auto fn = yz_kernel<Real, kYZThreads, R, C>;
+        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(yz_smem)));
+        if (d.csize > 8) RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        return cudaSuccess;
+    }
+    cudaError_t set_attributes() {
+        if (tw == 32) {
+            RB_CUDA_TRY((x_attr<32, true, false>()));
+            RB_CUDA_TRY((x_attr<32, true, true>()));
+            RB_CUDA_TRY((x_attr<32, false, true>()));
+            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem)));
+        } else {
+            RB_CUDA_TRY((x_attr<16, true, false>()));
+            RB_CUDA_TRY((x_attr<16, true, true>()));
+            RB_CUDA_TRY((x_attr<16, false, true>()));
+            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem)));
+        }
+        RB_CUDA_TRY((yz_attr<true, false>()));
+        RB_CUDA_TRY((yz_attr<true, true>()));
+        RB_CUDA_TRY((yz_attr<false, true>()));
+        return cudaSuccess;
+    }
+
+    template <bool R, bool C>
+    cudaError_t launch_x(const Real* xs, const Real* ys, const Real* zs, int step, int gate) {
+        if (tw == 32)
+            x_kernel<Real, 32, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
+        else
+            x_kernel<Real, 16, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
+        return cudaGetLastError();
+    }
+
+    template <bool R, bool C>
+    cudaError_t launch_yz(const Real* ys, const Real* zs, int step, int gate) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(tp * d.csize));
+        cfg.blockDim = dim3(kYZThreads);
+        cfg.dynamicSmemBytes = yz_smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(d.csize);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, yz_kernel<Real, kYZThreads, R, C>, d, ys, zs, step, gate);
+    }
+
+    cudaError_t launch_check(int mode) {
+        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.px, nbx, d.pyz, nbyz, d.pup, tp, d.plo,
+                                                   nblo, mode);
+        return cudaGetLastError();
+    }
+
+    // --- profiling ------------------------------------------------------
+    static constexpr int kKinds = 8;
+    std::vector<cudaEvent_t> evpool;
+    std::vector<std::pair<int, int>> marks;
+    bool profiling = false;
+    cudaError_t mark_begin(int kind) {
+        if (!profiling) return cudaSuccess;
+        const int idx = int(marks.size()) * 2;
+        while (int(evpool.size()) < idx + 2) {
+            cudaEvent_t ev;
+            RB_CUDA_TRY(cudaEventCreate(&ev));
+            evpool.push_back(ev);
+        }
+        marks.emplace_back(kind, idx);
+        return cudaEventRecord(evpool[idx], stream);
+    }
+    cudaError_t mark_end() {
+        if (!profiling) return cudaSuccess;
+        return cudaEventRecord(evpool[marks.back().second + 1], stream);
+    }
+#define RB_PTIMED(kind, expr)            \
+    do {                                 \
+        RB_CUDA_TRY(mark_begin(kind));   \
+        RB_CUDA_TRY(expr);               \
+        RB_CUDA_TRY(mark_end());         \
+    } while (0)
+
+    cudaError_t enqueue_block() {
+        const int op = p.op_steps;
+        for (int s = 0; s < op; ++s) {
+            if (s + 1 < op) {
+                RB_PTIMED(0, (launch_x<true, false>(d.xh, d.yh, d.zh, s, 0)));
+                RB_PTIMED(1, (launch_yz<true, false>(d.yh, d.zh, s, 0)));
+            } else {
+                RB_PTIMED(2, (launch_x<true, true>(d.xh, d.yh, d.zh, s, 0)));
+                RB_PTIMED(3, (launch_yz<true, true>(d.yh, d.zh, s, 0)));
+            }
+        }
+        RB_PTIMED(4, (upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.x2s, tp, 0), cudaGetLastError()));
+        RB_PTIMED(5, (lower_kernel<Real><<<nblo, kAuxThreads, 0, stream>>>(d, d.y2s, d.z2s), cudaGetLastError()));
+        RB_PTIMED(6, launch_check(1));
+        RB_PTIMED(7, (launch_x<false, true>(d.x2s, d.y2s, d.z2s, 0, 1)));
+        RB_PTIMED(7, (launch_yz<false, true>(d.y2s, d.z2s, 0, 1)));
+        RB_PTIMED(7, launch_check(2));
+        RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+        return cudaGetLastError();
+    }
+
+    cudaError_t capture_block() {
+        RB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t st = enqueue_block();
+        cudaError_t st2 = cudaStreamEndCapture(stream, &graph);
+        RB_CUDA_TRY(st);
+        RB_CUDA_TRY(st2);
+        return cudaGraphInstantiate(&exec, graph, 0);
+    }
+
+    cudaError_t launch_block() { return exec ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
+
+    int set_warm(const double* wx, const double* wy, const double* wz) override {
+        if (!wx || !wy || !wz) {
+            has_warm = false;
+            return 0;
+        }
+        const size_t full = size_t(n) * t * t;
+        if (warm[0].upload(wx, full, stream) || warm[1].upload(wy, full, stream) ||
+            warm[2].upload(wz, full, stream) || cudaStreamSynchronize(stream))
+            return int(cudaErrorMemoryAllocation);
+        has_warm = true;
+        return 0;
+    }
+
+    cudaError_t start_solve() {
+        nlaunch = 0;
+        // every run starts its thresholds cold (all-NaN bytes)
+        RB_CUDA_TRY(cudaMemsetAsync(thx.ptr, 0xFF, sizeof(double) * thx.count, stream));
+        RB_CUDA_TRY(cudaMemsetAsync(thy.ptr, 0xFF, sizeof(double) * thy.count, stream));
+        RB_CUDA_TRY(cudaMemsetAsync(thz.ptr, 0xFF, sizeof(double) * thz.count, stream));
+        init_kernel<Real><<<tp, 256, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
+        nlaunch += 1;
+        if (has_warm) {
+            warm_pack_kernel<Real><<<tp, 256, 0, stream>>>(d, warm[0].ptr, warm[1].ptr, warm[2].ptr, d.x0, d.y0,
+                                                           d.z0);
+            if (tw == 32)
+                project_x_kernel<Real, 32><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, d.x0);
+            else
+                project_x_kernel<Real, 16><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, d.x0);
+            project_yz_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.y0, d.z0);
+            nlaunch += 3;
+        }
+        // x1 = raw_step(x0): one vanilla step from the start point, with the
+        // sums for the error, and the bounds at the start point itself.
+        RB_CUDA_TRY(cudaGetLastError());
+        upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.x0, tp, 0);
+        lower_kernel<Real><<<nblo, kAuxThreads, 0, stream>>>(d, d.y0, d.z0);
+        RB_CUDA_TRY((launch_x<false, true>(d.x0, d.y0, d.z0, 0, 0)));
+        RB_CUDA_TRY((launch_yz<false, true>(d.y0, d.z0, 0, 0)));
+        RB_CUDA_TRY(launch_check(0));
+        RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+        nlaunch += 5;
+        return cudaStreamSynchronize(stream);
+    }
+
+    int run() override {
+        if (runs++ > 0 && !exec && capture_block() != cudaSuccess) return int(cudaErrorUnknown);
+        cudaError_t st = start_solve();
+        if (st != cudaSuccess) return int(st);
+        if (!mirror->terminated) {
+            for (int kk = 0; kk < 2; ++kk) {
+                if ((st = launch_block()) != cudaSuccess) return int(st);
+                if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
+                nlaunch += block_nodes;
+            }
+            int kk = 0;
+            for (;;) {
+                if ((st = cudaEventSynchronize(done[kk])) != cudaSuccess) return int(st);
+                if (mirror->terminated) break;
+                if (p.verbose)
+                    fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e\n",
+                            mirror->iteration, mirror->upper, mirror->lower, mirror->gap);
+                if ((st = launch_block()) != cudaSuccess) return int(st);
+                if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
+                nlaunch += block_nodes;
+                kk ^= 1;
+            }
+        }
+        if ((st = cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (st = cudaStreamSynchronize(stream)) != cudaSuccess)
+            return int(st);
+        return 0;
+    }
+
+    int run_profiled(double* ms, long long* count) override {
+        for (int kk = 0; kk < kKinds; ++kk) { ms[kk] = 0.0; count[kk] = 0; }
+        cudaError_t st = start_solve();
+        if (st != cudaSuccess) return int(st);
+        profiling = true;
+        while (!mirror->terminated) {
+            marks.clear();
+            if ((st = enqueue_block()) != cudaSuccess || (st = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                profiling = false;
+                return int(st);
+            }
+            nlaunch += block_nodes;
+            for (auto& mk : marks) {
+                float tm = 0.f;
+                if ((st = cudaEventElapsedTime(&tm, evpool[mk.second], evpool[mk.second + 1])) != cudaSuccess) {
+                    profiling = false;
+                    return int(st);
+                }
+                ms[mk.first] += tm;
+                count[mk.first] += 1;
+            }
+        }
+        profiling = false;
+        if ((st = cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (st = cudaStreamSynchronize(stream)) != cudaSuccess)
+            return int(st);
+        return 0;
+    }
+
+    // The objective at the returned (unpadded) x, in instance units.
+    cudaError_t final_primal(double* out) {
+        const Real* xs = mirror->result_slot == 1 ? d.x0 : d.x2s;
+        Dev<Real> dd = d;
+        dd.pup = final_up.ptr;
+        upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(dd, xs, t, 1);
+        std::vector<double> host(size_t(tp) * 3);
+        RB_CUDA_TRY(cudaMemcpyAsync(host.data(), final_up.ptr, sizeof(double) * host.size(),
+                                    cudaMemcpyDeviceToHost, stream));
+        RB_CUDA_TRY(cudaStreamSynchronize(stream));
+        double sum = 0.0;
+        for (double v : host) sum += v;
+        *out = sum * prm.scale;
+        return cudaSuccess;
+    }
+
+    template <class Out>
+    cudaError_t unpack(const Real* src, int mode, Out* host) {
+        PoolBuf<Out> buf;
+        const size_t full = size_t(n) * t * t;
+        RB_CUDA_TRY(buf.alloc(full, stream));
+        unpack_kernel<Real, Out><<<1184, 256, 0, stream>>>(d, src, mode, buf.ptr);
+        RB_CUDA_TRY(cudaMemcpyAsync(host, buf.ptr, sizeof(Out) * full, cudaMemcpyDeviceToHost, stream));
+        return cudaStreamSynchronize(stream);
+    }
+
+    template <class Out>
+    int result_t(Out* x, Out* y, Out* z, pria_result_info* info) {
+        const bool start = mirror->result_slot == 1;
+        const Real* xs = start ? d.x0 : d.x2s;
+        const Real* ys = start ? d.y0 : d.y2s;
+        const Real* zs = start ? d.z0 : d.z2s;
+        cudaError_t st;
+        if (x && (st = unpack<Out>(xs, 0, x)) != cudaSuccess) return int(st);
+        if (y && (st = unpack<Out>(ys, 1, y)) != cudaSuccess) return int(st);
+        if (z && (st = unpack<Out>(zs, 2, z)) != cudaSuccess) return int(st);
+        if (info) {
+            double primal = 0.0;
+            if ((st = final_primal(&primal)) != cudaSuccess) return int(st);
+            info->iterations = mirror->iteration;
+            info->primal_objective = primal;
+            info->dual_objective = mirror->lower;
+            info->relative_gap = (primal - mirror->lower) / (1.0 + std::fabs(primal) + std::fabs(mirror->lower));
+        }
+        return 0;
+    }
+    int result(double* x, double* y, double* z, pria_result_info* info) override {
+        return result_t<double>(x, y, z, info);
+    }
+    int result_f32(float* x, float* y, float* z, pria_result_info* info) override {
+        return result_t<float>(x, y, z, info);
+    }
+
+    long long launches() const override { return nlaunch; }
+
+    size_t device_bytes() const {
+        size_t b = 0;
+        for (auto* x : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s})
+            b += x->count * sizeof(Real);
+        for (auto* x : {&px, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b += x->count * sizeof(double);
+        return b + sizeof(Control);
+    }
+};
+
+template <class In>
+static int create(int64_t n, int64_t t, const In* K, double K0, const In* H, const pria_params* params,
+                  int use_float32, cudaStream_t stream, std::unique_ptr<SolverBase>& out) {
+    if (n < 1 || t < 1 || !K || !H || !params) return int(cudaErrorInvalidValue);
+    const int64_t tp = t + (t & 1);
+    if (tp > kMaxPeriods || n > (1LL << 24)) return int(cudaErrorInvalidValue);
+    pria_params p = *params;
+    if (p.op_steps < 2) p.op_steps = 2;
+    if (p.warm_steps < 0) p.warm_steps = 0;
+    if (!p.use_halpern || p.warm_steps > 0) {
+        // the vanilla loop (and the warm phase) of solver.py:601-606 is not
+        // built: only the restarted Halpern method with warm_steps = 0
+        return int(cudaErrorNotSupported);
+    }
+    if (p.max_iter < 0) p.max_iter = -1;
+    cudaError_t st;
+    if (use_float32) {
+        auto* s = new Solver<float>();
+        out.reset(s);
+        s->p = p;
+        st = s->template setup<In>(n, t, K, K0, H, stream);
+    } else {
+        auto* s = new Solver<double>();
+        out.reset(s);
+        s->p = p;
+        st = s->template setup<In>(n, t, K, K0, H, stream);
+    }
+    return int(st);
+}
+
+}  // namespace
+}  // namespace pria
+}  // namespace rb200
