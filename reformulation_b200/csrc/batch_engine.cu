@@ -21,6 +21,7 @@
 #include "pria_core.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -256,12 +257,15 @@ struct Engine final : EngineBase {
         std::unique_ptr<praq::Solver<Real>> s;
         bool started = false, done = false, live = true;
         Summary last{};
+        long long join = 0;   // the first block that includes it
     };
     struct JInst {
         std::unique_ptr<pria::Solver<Real>> s;
         bool started = false, done = false, live = true;
         Summary last{};
+        long long join = 0;
     };
+    long long launched = 0, synced = 0;   // blocks enqueued / inspected so far
     std::vector<QInst> q;
     std::vector<JInst> j;
     std::vector<std::pair<int, int>> ids;   // id -> (0 QUBO / 1 JRP, index)
@@ -474,6 +478,7 @@ struct Engine final : EngineBase {
             hsummary = nullptr;
             if (cudaMallocHost(reinterpret_cast<void**>(&hsummary), sizeof(Summary) * summary.count))
                 return -int(cudaErrorMemoryAllocation);
+            std::memset(hsummary, 0, sizeof(Summary) * summary.count);
             hsummary_cap = summary.count;
         }
         // (host-to-device copies from pageable memory are staged when issued)
@@ -623,6 +628,7 @@ struct Engine final : EngineBase {
             const int st = qi.s->start_solve();
             if (st) return st;
             qi.started = true;
+            qi.join = launched;
             nlaunch += qi.s->launches();
             qi.done = qi.s->mirror->terminated != 0;
             const auto* c = qi.s->mirror;
@@ -633,6 +639,7 @@ struct Engine final : EngineBase {
             const cudaError_t st = ji.s->start_solve();
             if (st) return -int(st);
             ji.started = true;
+            ji.join = launched;
             nlaunch += ji.s->launches();
             ji.done = ji.s->mirror->terminated != 0;
             const auto* c = ji.s->mirror;
@@ -658,6 +665,7 @@ struct Engine final : EngineBase {
         if (cudaGraphLaunch(exec, stream)) return -int(cudaErrorUnknown);
         if (cudaEventRecord(events[(head + pending) % events.size()], stream)) return -int(cudaErrorUnknown);
         ++pending;
+        ++launched;
         nlaunch += block_nodes;
         return 0;
     }
@@ -666,6 +674,7 @@ struct Engine final : EngineBase {
     int drain() {
         if (cudaStreamSynchronize(stream)) return -1;
         head = (head + pending) % int(events.size());
+        synced += pending;
         pending = 0;
         return 0;
     }
@@ -676,6 +685,7 @@ struct Engine final : EngineBase {
         if (cudaEventSynchronize(events[head])) return -int(cudaErrorUnknown);
         head = (head + 1) % int(events.size());
         --pending;
+        const long long block = synced++;
         // the host copy holds the state after this block (or a later one)
         bool changed = false;
         int nout = 0;
@@ -686,6 +696,8 @@ struct Engine final : EngineBase {
             const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
                                            : (j[k].s && j[k].started && !j[k].done);
             if (!running) continue;
+            // only blocks enqueued after the instance joined carry its state
+            if (block < (kind == 0 ? q[k].join : j[k].join)) continue;
             const Summary s = hsummary[slot];
             (kind == 0 ? q[k].last : j[k].last) = s;
             if (s.terminated) {
