@@ -57,6 +57,14 @@ REFORM_API int reform_batch_add_jrp(reform_batch* b, int64_t n, int64_t t, const
                                     double joint_cost, const double* holding_costs,
                                     const pria_params* params);
 
+/* A JRP whose holding costs are demand-driven, H_ist = rate_i d_it (t - s)
+ * for s <= t (rate [n], demand [n][t]): the same LP as reform_batch_add_jrp
+ * with that dense H, given in N + N T numbers instead of N T^2; the packed
+ * costs are built on the device. */
+REFORM_API int reform_batch_add_jrp_demand(reform_batch* b, int64_t n, int64_t t, const double* order_costs,
+                                           double joint_cost, const double* rate, const double* demand,
+                                           const pria_params* params);
+
 /* Cold-start every instance added since the last call (the first vanilla step
  * and the check before the loop) and put it in the work tables. */
 REFORM_API int reform_batch_start(reform_batch* b);
@@ -95,6 +103,10 @@ REFORM_API int64_t reform_batch_device_bytes(const reform_batch* b);
  * keep the fastest; `out` receives the choice. */
 REFORM_API int reform_batch_set_shapes(reform_batch* b, const reform_shapes* shapes);
 REFORM_API int reform_batch_autotune(reform_batch* b, reform_shapes* out);
+
+/* Cold-start every instance that is still held (done or not) again: the
+ * instances stay laid out on the device, their iterates start over. */
+REFORM_API int reform_batch_restart(reform_batch* b);
 
 /* Kernel launches issued by the engine since creation (graph nodes counted). */
 REFORM_API int64_t reform_batch_launches(const reform_batch* b);

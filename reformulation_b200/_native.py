@@ -107,6 +107,7 @@ def _declare(lib):
         "reform_batch_create": (I, [I, V, P(V)]),
         "reform_batch_add_qubo": (I, [V, P(PraqInstance), P(PraqParameters)]),
         "reform_batch_add_jrp": (I, [V, c_int64, c_int64, D, c_double, D, P(PriaParams)]),
+        "reform_batch_add_jrp_demand": (I, [V, c_int64, c_int64, D, c_double, D, D, P(PriaParams)]),
         "reform_batch_start": (I, [V]),
         "reform_batch_run": (I, [V, c_int64]),
         "reform_batch_launch": (I, [V]),
@@ -119,6 +120,7 @@ def _declare(lib):
         "reform_batch_device_bytes": (c_int64, [V]),
         "reform_batch_set_shapes": (I, [V, P(ReformShapes)]),
         "reform_batch_autotune": (I, [V, P(ReformShapes)]),
+        "reform_batch_restart": (I, [V]),
         "reform_batch_launches": (c_int64, [V]),
         "reform_batch_destroy": (None, [V]),
     })

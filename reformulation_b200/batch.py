@@ -49,6 +49,21 @@ class Batch:
         self.kinds[id_] = ("jrp", instance)
         return id_
 
+    def add_jrp_demand(self, spec, parameters=None) -> int:
+        """A demand-form JRP (instances.JrpSpec: K, K0, rates h_i, demands
+        d_it), the packed holding costs built on the device."""
+        k = np.ascontiguousarray(spec.order_costs, np.float64)
+        rate = np.ascontiguousarray(spec.holding_rate, np.float64)
+        demand = np.ascontiguousarray(spec.demand, np.float64)
+        p = parameters or self._lib.pria_params_auto(-1, 1e-8)
+        id_ = self._lib.reform_batch_add_jrp_demand(self._h, spec.items, spec.periods, _native.dptr(k),
+                                                    float(spec.joint_order_cost), _native.dptr(rate),
+                                                    _native.dptr(demand), ctypes.byref(p))
+        if id_ < 0:
+            raise RuntimeError(f"reform_batch_add_jrp_demand failed with status {id_}")
+        self.kinds[id_] = ("jrp", spec)
+        return id_
+
     def start(self) -> None:
         st = self._lib.reform_batch_start(self._h)
         if st != 0:
@@ -128,6 +143,12 @@ class Batch:
             raise RuntimeError(f"reform_batch_autotune failed with status {st}")
         return {"praq_half_edges_per_lane": s.praq_half_edges_per_lane,
                 "grid_multiplier": s.grid_multiplier}
+
+    def restart(self) -> None:
+        """Cold-start every held instance again (the layouts stay resident)."""
+        st = self._lib.reform_batch_restart(self._h)
+        if st != 0:
+            raise RuntimeError(f"reform_batch_restart failed with status {st}")
 
     def launches(self) -> int:
         return int(self._lib.reform_batch_launches(self._h))

@@ -229,6 +229,8 @@ struct EngineBase {
     virtual int add_qubo(const PraqInstance& in, const PraqParameters& p) = 0;
     virtual int add_jrp(int64_t n, int64_t t, const double* k, double k0, const double* h,
                         const pria_params& p) = 0;
+    virtual int add_jrp_demand(int64_t n, int64_t t, const double* k, double k0, const double* rate,
+                               const double* demand, const pria_params& p) = 0;
     virtual int start() = 0;
     virtual int run(int64_t max_blocks) = 0;
     virtual int launch() = 0;
@@ -242,6 +244,7 @@ struct EngineBase {
     virtual int set_shapes(const reform_shapes& s) = 0;
     virtual int autotune(reform_shapes* out) = 0;
     virtual int64_t launches() const = 0;
+    virtual int restart() = 0;
 };
 
 template <class Real>
@@ -302,12 +305,25 @@ struct Engine final : EngineBase {
         for (auto ev : events) cudaEventDestroy(ev);
         q.clear();
         j.clear();
-        if (hsummary) cudaFreeHost(hsummary);
+        // every stream-ordered free before the stream goes away
+        qdevs.buf.release();
+        qmeta.buf.release();
+        jdevs.buf.release();
+        jmeta.buf.release();
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow}) tb->buf.release();
+        for (auto& tb : t_yz) tb.buf.release();
+        l_qcheck.buf.release();
+        l_jcheck.buf.release();
+        live.buf.release();
+        counts.release();
+        summary.release();
         if (stream) cudaStreamSynchronize(stream);
+        if (hsummary) cudaFreeHost(hsummary);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
     int init(cudaStream_t s) {
+        (void)cudaGetLastError();   // a stale error of an unrelated earlier call is not ours
         if (s) {
             stream = s;
         } else {
@@ -348,6 +364,21 @@ struct Engine final : EngineBase {
         p.op_steps = op_steps;
         std::unique_ptr<pria::SolverBase> base;
         const int st = pria::create<double>(n, t, k, k0, h, &p, sizeof(Real) == 4, stream, base);
+        if (st) return -st;
+        std::unique_ptr<pria::Solver<Real>> s(static_cast<pria::Solver<Real>*>(base.release()));
+        j.push_back(JInst{std::move(s)});
+        ids.emplace_back(1, int(j.size()) - 1);
+        dirty = true;
+        return int(ids.size()) - 1;
+    }
+
+    int add_jrp_demand(int64_t n, int64_t t, const double* k, double k0, const double* rate, const double* demand,
+                       const pria_params& p0) override {
+        pria_params p = p0;
+        if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
+        p.op_steps = op_steps;
+        std::unique_ptr<pria::SolverBase> base;
+        const int st = pria::create_demand(n, t, k, k0, rate, demand, &p, sizeof(Real) == 4, stream, base);
         if (st) return -st;
         std::unique_ptr<pria::Solver<Real>> s(static_cast<pria::Solver<Real>*>(base.release()));
         j.push_back(JInst{std::move(s)});
@@ -802,7 +833,9 @@ struct Engine final : EngineBase {
         return rc ? rc : rebuild();
     }
 
-    // Restart every started instance from its cold start (used by the tuner).
+    int restart() override { return restart_all(); }
+
+    // Restart every instance from its cold start (the tuner, repeated solves).
     int restart_all() {
         if (pending && drain()) return -1;
         for (auto& qi : q) if (qi.s) qi.started = qi.done = false;
@@ -926,6 +959,12 @@ int reform_batch_add_jrp(reform_batch* b, int64_t n, int64_t t, const double* k,
     return b->impl->add_jrp(n, t, k, k0, h, *params);
 }
 
+int reform_batch_add_jrp_demand(reform_batch* b, int64_t n, int64_t t, const double* k, double k0,
+                                const double* rate, const double* demand, const pria_params* params) {
+    if (!b || !params) return -int(cudaErrorInvalidValue);
+    return b->impl->add_jrp_demand(n, t, k, k0, rate, demand, *params);
+}
+
 int reform_batch_start(reform_batch* b) { return b ? b->impl->start() : PRAQ_ERROR_ARGUMENT; }
 int reform_batch_run(reform_batch* b, int64_t max_blocks) { return b ? b->impl->run(max_blocks) : PRAQ_ERROR_ARGUMENT; }
 int reform_batch_launch(reform_batch* b) { return b ? b->impl->launch() : PRAQ_ERROR_ARGUMENT; }
@@ -948,6 +987,7 @@ int reform_batch_set_shapes(reform_batch* b, const reform_shapes* s) {
     return b && s ? b->impl->set_shapes(*s) : PRAQ_ERROR_ARGUMENT;
 }
 int reform_batch_autotune(reform_batch* b, reform_shapes* out) { return b ? b->impl->autotune(out) : PRAQ_ERROR_ARGUMENT; }
+int reform_batch_restart(reform_batch* b) { return b ? b->impl->restart() : PRAQ_ERROR_ARGUMENT; }
 int64_t reform_batch_launches(const reform_batch* b) { return b ? b->impl->launches() : 0; }
 void reform_batch_destroy(reform_batch* b) { delete b; }
 

@@ -44,6 +44,7 @@ int reform_praq_create(const PraqInstance* instance, const PraqParameters* param
                        void* stream, reform_praq_solver** out) {
     if (out) *out = nullptr;
     if (!instance || !parameters || !out) return PRAQ_ERROR_ARGUMENT;
+    (void)cudaGetLastError();   // a stale error of an unrelated earlier call is not ours
     PraqParameters p = *parameters;
     if (!praq::valid(p)) return PRAQ_ERROR_ARGUMENT;
     const int64_t limit = std::numeric_limits<int>::max();

@@ -824,6 +824,23 @@ __global__ void h_pack_kernel(Dev<Real> d, const In* __restrict__ H, double inv_
     }
 }
 
+// Demand-form holding costs: h[i, s, t] = rate_i d_it (t - s) / scale for
+// s <= t < T, zero on the pad period.
+template <class Real>
+__global__ void h_demand_kernel(Dev<Real> d, const double* __restrict__ rate, const double* __restrict__ demand,
+                                double inv_scale, Real* __restrict__ h) {
+    const int s = blockIdx.x;
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const long long count = (long long)d.n * len;
+    for (long long q = threadIdx.x; q < count; q += blockDim.x) {
+        const int i = int(q / len), t = s + int(q % len);
+        double v = 0.0;
+        if (s < d.t && t < d.t) v = rate[i] * demand[(long long)i * d.t + t] * double(t - s) * inv_scale;
+        h[base + q] = Real(v);
+    }
+}
+
 constexpr int kSquareBlocks = 296;
 
 __global__ void sum_rows_kernel(const double* __restrict__ partial, int count, double* out) {
@@ -885,8 +902,8 @@ struct Solver final : SolverBase {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
-    template <class In>
-    cudaError_t setup(int64_t n_, int64_t t_, const In* K, double K0, const In* H, cudaStream_t s) {
+    cudaError_t begin(int64_t n_, int64_t t_, cudaStream_t s) {
+        (void)cudaGetLastError();   // a stale error of an unrelated earlier call is not ours
         n = int(n_);
         t = int(t_);
         tp = t + (t & 1);
@@ -899,6 +916,54 @@ struct Solver final : SolverBase {
         }
         mirror = static_cast<Control*>(pinned_get());
         if (!mirror) return cudaErrorMemoryAllocation;
+        return cudaSuccess;
+    }
+
+    // The scaled K on the device and the scalar fields of the descriptor.
+    template <class In>
+    cudaError_t set_costs(const In* K, double K0, double hsq) {
+        double ss = K0 * K0 + hsq;
+        for (int i = 0; i < n; ++i) ss += double(K[i]) * double(K[i]);
+        prm.scale = ss > 0.0 ? std::sqrt(ss) : 1.0;
+        std::vector<Real> ks(n);
+        for (int i = 0; i < n; ++i) ks[i] = Real(double(K[i]) / prm.scale);
+        RB_CUDA_TRY(k.upload(ks.data(), n, stream));
+        RB_CUDA_TRY(h.alloc(nd, stream));
+        d.n = n; d.t = t; d.tp = tp; d.nd = nd;
+        d.k = k.ptr;
+        d.k0 = Real(K0 / prm.scale);
+        return cudaSuccess;
+    }
+
+    // Demand-form holding costs H_ist = rate_i d_it (t - s): the packed h is
+    // built on the device from N + N T numbers, and sum H^2 on the host as
+    // sum_i rate_i^2 sum_t d_it^2 sum_{s<=t} (t - s)^2.
+    cudaError_t setup_demand(int64_t n_, int64_t t_, const double* K, double K0, const double* rate,
+                             const double* demand, cudaStream_t s) {
+        RB_CUDA_TRY(begin(n_, t_, s));
+        double hsq = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int tt = 0; tt < t; ++tt) {
+                const double dd = demand[(long long)i * t + tt], lag = double(tt);
+                acc += dd * dd * (lag * (lag + 1.0) * (2.0 * lag + 1.0) / 6.0);
+            }
+            hsq += rate[i] * rate[i] * acc;
+        }
+        RB_CUDA_TRY(set_costs<double>(K, K0, hsq));
+        {
+            PoolBuf<double> rd, dd;
+            RB_CUDA_TRY(rd.upload(rate, n, stream));
+            RB_CUDA_TRY(dd.upload(demand, size_t(n) * t, stream));
+            h_demand_kernel<Real><<<tp, 256, 0, stream>>>(d, rd.ptr, dd.ptr, 1.0 / prm.scale, h.ptr);
+            RB_CUDA_TRY(cudaGetLastError());
+        }
+        return setup_common();
+    }
+
+    template <class In>
+    cudaError_t setup(int64_t n_, int64_t t_, const In* K, double K0, const In* H, cudaStream_t s) {
+        RB_CUDA_TRY(begin(n_, t_, s));
         // scale = ||(triu H, K, K0)||_2 (solver.py:652-654)
         double hsq = 0.0;
         {
@@ -913,19 +978,15 @@ struct Solver final : SolverBase {
             RB_CUDA_TRY(cudaMemcpyAsync(hp, tot.ptr, sizeof(double), cudaMemcpyDeviceToHost, stream));
             RB_CUDA_TRY(cudaStreamSynchronize(stream));
             hsq = *hp;
-            double ss = K0 * K0 + hsq;
-            for (int i = 0; i < n; ++i) ss += double(K[i]) * double(K[i]);
-            prm.scale = ss > 0.0 ? std::sqrt(ss) : 1.0;
-            std::vector<Real> ks(n);
-            for (int i = 0; i < n; ++i) ks[i] = Real(double(K[i]) / prm.scale);
-            RB_CUDA_TRY(k.upload(ks.data(), n, stream));
-            RB_CUDA_TRY(h.alloc(nd, stream));
-            d.n = n; d.t = t; d.tp = tp; d.nd = nd;
-            d.k = k.ptr;
-            d.k0 = Real(K0 / prm.scale);
+            RB_CUDA_TRY(set_costs<In>(K, K0, hsq));
             h_pack_kernel<In, Real><<<tp, 256, 0, stream>>>(d, Hd.ptr, 1.0 / prm.scale, h.ptr);
             RB_CUDA_TRY(cudaGetLastError());
         }
+        return setup_common();
+    }
+
+    // Everything after h: iterates, partial rows, tiles, cluster size.
+    cudaError_t setup_common() {
         for (auto* b : {&xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s})
             RB_CUDA_TRY(b->alloc(nd, stream));
         tw = sizeof(Real) == 4 ? 32 : 16;
@@ -1287,6 +1348,31 @@ static int create(int64_t n, int64_t t, const In* K, double K0, const In* H, con
         out.reset(s);
         s->p = p;
         st = s->template setup<In>(n, t, K, K0, H, stream);
+    }
+    return int(st);
+}
+
+static int create_demand(int64_t n, int64_t t, const double* K, double K0, const double* rate,
+                         const double* demand, const pria_params* params, int use_float32, cudaStream_t stream,
+                         std::unique_ptr<SolverBase>& out) {
+    if (n < 1 || t < 1 || !K || !rate || !demand || !params) return int(cudaErrorInvalidValue);
+    const int64_t tp = t + (t & 1);
+    if (tp > kMaxPeriods || n > (1LL << 24)) return int(cudaErrorInvalidValue);
+    pria_params p = *params;
+    if (p.op_steps < 2) p.op_steps = 2;
+    if (!p.use_halpern || p.warm_steps > 0) return int(cudaErrorNotSupported);
+    if (p.max_iter < 0) p.max_iter = -1;
+    cudaError_t st;
+    if (use_float32) {
+        auto* s = new Solver<float>();
+        out.reset(s);
+        s->p = p;
+        st = s->setup_demand(n, t, K, K0, rate, demand, stream);
+    } else {
+        auto* s = new Solver<double>();
+        out.reset(s);
+        s->p = p;
+        st = s->setup_demand(n, t, K, K0, rate, demand, stream);
     }
     return int(st);
 }
