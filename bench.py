@@ -396,6 +396,202 @@ def run_ours(args):
     return 0
 
 
+def _timed_events(torch, stream):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_pria(args):
+    """Config 3: one JRP LP, N = 100 items, T = 500 periods (seed 2), to 1e-4,
+    mixed precision beside plain FP64; one step = one solve from the cold
+    start on the resident instance."""
+    import torch
+
+    from reformulation_b200 import pria
+    from reformulation_b200.instances import jrp_demand
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    inst = jrp_demand(2, 100, 500)
+    lib = pria.Library()
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for prec in ("mixed", "fp64"):
+        dev = pria.DeviceSolver(inst, lib.parameters(1_000_000, TOL), prec, stream=stream.cuda_stream)
+        for _ in range(args.warmup):
+            dev.run()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = _timed_events(torch, stream)
+            a.record(stream)
+            dev.run()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        r = dev.result()
+        _, prof = dev.run_profiled()
+        real = 4 if prec == "mixed" else 8
+        nd = 100 * 500 * 501 // 2
+        per = {k: v[0] / v[1] for k, v in prof.items() if v[1]}
+        out[prec] = {"solves_per_s": 1e3 * len(ms) / sum(ms), "p50_ms": float(np.percentile(ms, 50)),
+                     "p99_ms": float(np.percentile(ms, 99)), "iterations": r.iterations,
+                     "relative_gap": r.relative_gap, "upper": r.primal_objective,
+                     "kernels_ms_per_launch": per,
+                     "x_kernel_gbs": 7 * nd * real / (per["x"] / 1e3) / 1e9,
+                     "yz_kernel_gbs": 7 * nd * real / (per["yz"] / 1e3) / 1e9}
+        dev.close()
+    line = {"metric": METRIC, "workload": "PRIA JRP LP N=100 T=500 (seed 2), demand-driven H, to 1e-4",
+            "value": out["mixed"]["solves_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "mixed": out["mixed"], "plain_fp64": out["fp64"],
+            "mixed_vs_fp64": out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"],
+            "peak_hbm_gbs": peaks()[0], "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args):
+    """Config 4: 256 QUBO + 128 JRP of log-uniform sizes (seed 3) in one
+    engine, mixed precision, to 1e-4; one step = a cold restart and a full
+    solve of all 384 instances, resident on the device.  The plain FP64
+    single-instance kernel is timed on a sample of the same instances (every
+    `--fp64-stride`-th one, each solved alone, device-resident) and scaled to
+    the whole set."""
+    import torch
+
+    from reformulation_b200 import praq, pria
+    from reformulation_b200.batch import Batch
+    from reformulation_b200.instances import batch_mix
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    t_gen = time.perf_counter()
+    qs, js = batch_mix(3, args.qubos, args.jrps)
+    t_gen = time.perf_counter() - t_gen
+    ql, jl = praq.Library(), pria.Library()
+    qp = ql.parameters(tolerance=TOL, max_iter=1_000_000, use_float32=1)
+    jp = jl.parameters(1_000_000, TOL)
+    b = Batch("mixed", stream=stream.cuda_stream)
+    t_lay = time.perf_counter()
+    ids = [b.add_qubo(q, qp) for q in qs] + [b.add_jrp_demand(j, jp) for j in js]
+    b.start()
+    t_lay = time.perf_counter() - t_lay
+    shapes = b.autotune() if args.autotune else None
+    for _ in range(args.warmup):
+        b.restart()
+        b.run()
+    ms = []
+    launches0 = b.launches()
+    for _ in range(args.steps):
+        b.restart()
+        a, e = _timed_events(torch, stream)
+        a.record(stream)
+        b.run()
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(e))
+    launches = b.launches() - launches0
+    its = []
+    gaps = []
+    for i in ids:
+        done, it, lo, up = b.status(i)
+        its.append(it)
+        gaps.append((up - lo) / (1 + abs(up) + abs(lo)))
+    total = len(ids)
+    value = 1e3 * total * len(ms) / sum(ms)
+    # plain FP64 single-instance kernel on a sample
+    sample = list(range(0, total, args.fp64_stride))
+    fp64_ms = []
+    for k in sample:
+        if k < len(qs):
+            dev = praq.DeviceSolver(qs[k], ql.parameters(tolerance=TOL, max_iter=1_000_000),
+                                    stream=stream.cuda_stream)
+        else:
+            dev = pria.DeviceSolver(js[k - len(qs)].build(), jl.parameters(1_000_000, TOL), "fp64",
+                                    stream=stream.cuda_stream)
+        dev.run()
+        a, e = _timed_events(torch, stream)
+        a.record(stream)
+        dev.run()
+        e.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms.append(a.elapsed_time(e))
+        dev.close()
+    fp64_value = 1e3 * len(fp64_ms) / sum(fp64_ms)
+    line = {"metric": METRIC, "workload": f"batch {len(qs)} QUBO + {len(js)} JRP (seed 3), to 1e-4",
+            "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sum(ms) / len(ms), "dtype": "f32 iterates, f64 reductions",
+            "instances": total, "max_gap": max(gaps), "iterations_p50": float(np.percentile(its, 50)),
+            "iterations_max": int(max(its)), "device_bytes": b.device_bytes(), "shapes": shapes,
+            "gpu_launches": int(launches),
+            "plain_fp64_sequential": {"value": fp64_value, "unit": UNIT, "sample": len(sample),
+                                      "sample_stride": args.fp64_stride},
+            "batched_vs_plain_fp64": value / fp64_value,
+            "generate_s": t_gen, "layout_s": t_lay, "data": "synthetic"}
+    b.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args):
+    """Config 5: Poisson arrivals (seed 4) at each rate of --rates for
+    --seconds, 70 % QUBO / 30 % JRP, instances drawn from a pool of the
+    config-4 size distributions; HBM admission budget 150 GB.  Latency =
+    arrival to result on the host.  Comparator: the same arrival stream served
+    FIFO by the plain FP64 single-instance solver (its measured end-to-end time
+    per pool instance)."""
+    import torch
+
+    from reformulation_b200 import serving
+    from reformulation_b200.instances import _jrp_log_uniform, _qubo_log_uniform
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(4)
+    pool_q = [_qubo_log_uniform(rng, k, 4) for k in range(args.pool_qubo)]
+    pool_j = [_jrp_log_uniform(rng, k, 4) for k in range(args.pool_jrp)]
+    svc = serving.service_times_fp64(pool_q + pool_j, TOL)
+    svc_q, svc_j = svc[:len(pool_q)], svc[len(pool_q):]
+    rows = []
+    for rate in args.rates:
+        arr = np.random.default_rng(4)
+        reqs, kinds, t = [], [], 0.0
+        k = 0
+        while True:
+            t += float(arr.exponential(1.0 / rate))
+            if t > args.seconds:
+                break
+            if arr.random() < 0.7:
+                idx = int(arr.integers(len(pool_q)))
+                reqs.append(serving.Request(k, t, pool_q[idx]))
+                kinds.append(svc_q[idx])
+            else:
+                idx = int(arr.integers(len(pool_j)))
+                reqs.append(serving.Request(k, t, pool_j[idx]))
+                kinds.append(svc_j[idx])
+            k += 1
+        server = serving.Server(budget_bytes=150e9, tolerance=TOL)
+        t0 = time.perf_counter()
+        done = server.serve(reqs, t0=t0)
+        wall = max(c.finished for c in done) if done else 0.0
+        lat = [c.latency for c in done]
+        seq = serving.sequential_fifo([r.arrival for r in reqs], kinds)
+        seq_wall = max(r.arrival for r in reqs) + 0.0
+        free = 0.0
+        for a, s in sorted(zip([r.arrival for r in reqs], kinds)):
+            free = max(a, free) + s
+        rows.append({"rate": rate, "requests": len(reqs), "solves_per_s": len(done) / wall,
+                     **{f"{q}_ms": 1e3 * v for q, v in serving.percentiles(lat).items()},
+                     "max_gap": max(c.gap for c in done), "hbm_high_water_gb": server.high_water / 1e9,
+                     "plain_fp64_fifo": {"solves_per_s": len(reqs) / free,
+                                         **{f"{q}_ms": 1e3 * v for q, v in serving.percentiles(seq).items()}}})
+        server.close()
+        del seq_wall
+    line = {"metric": METRIC, "workload": "serving: Poisson arrivals, 70% QUBO / 30% JRP (seed 4)",
+            "unit": UNIT, "n_gpus": 1, "seconds_per_rate": args.seconds,
+            "pool": {"qubo": len(pool_q), "jrp": len(pool_j)}, "rates": rows, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,11 +599,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    ap.add_argument("--workload", choices=("praq", "pria", "batch", "serving"), default="praq",
+                    help="praq (the default line); pria, batch and serving measure the other configs")
+    ap.add_argument("--qubos", type=int, default=256)
+    ap.add_argument("--jrps", type=int, default=128)
+    ap.add_argument("--fp64-stride", type=int, default=12)
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--rates", type=float, nargs="+", default=[50, 100, 200, 500, 1000, 2000])
+    ap.add_argument("--seconds", type=float, default=2.0)
+    ap.add_argument("--pool-qubo", type=int, default=28)
+    ap.add_argument("--pool-jrp", type=int, default=12)
     args = ap.parse_args()
+    if args.impl == "reference":
+        if args.warmup < 3:
+            args.warmup = 3
+        return run_reference(args)
+    if args.workload == "pria":
+        return run_pria(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
-        return run_reference(args)
     return run_ours(args)
 
 
