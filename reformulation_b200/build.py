@@ -6,6 +6,9 @@ Run as ``python -m reformulation_b200.build`` (or through
 ``__graft_entry__.build()``).  Incremental: a source newer than the library
 triggers a rebuild of the whole library (the sources are few and nvcc runs per
 file in parallel).
+
+The file CLIs of cli/ (praq_solve_file, pria_solve_file: host C++ over the C
+ABI) are linked against the library into the same folder, with an rpath to it.
 """
 
 from __future__ import annotations
@@ -23,6 +26,8 @@ CSRC = PKG / "csrc"
 OUT = PKG / "_lib"
 LIB = OUT / "libreform_b200.so"
 OBJ = OUT / "obj"
+CLI_SRC = PKG / "cli"
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
@@ -65,8 +70,32 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
+def cli_targets() -> list[tuple[Path, Path]]:
+    return [(src, OUT / src.stem) for src in sorted(CLI_SRC.glob("*.cpp"))]
+
+
+def build_cli(force: bool = False) -> list[Path]:
+    """Link each cli/*.cpp against the library (host code only: g++)."""
+    out = []
+    cxx = shutil.which("g++") or "g++"
+    for src, exe in cli_targets():
+        deps = [src, LIB] + sorted((ROOT / "include").glob("*.h"))
+        if not force and exe.exists() and all(d.stat().st_mtime <= exe.stat().st_mtime for d in deps):
+            out.append(exe)
+            continue
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", f"-I{CUDA_HOME / 'include'}",
+               str(src), "-o", str(exe), f"-L{OUT}", "-lreform_b200", f"-L{CUDA_HOME / 'lib64'}", "-lcudart",
+               "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME / 'lib64'}"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"building {src.name} failed:\n{res.stderr}")
+        out.append(exe)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not stale():
+        build_cli()
         return LIB
     OBJ.mkdir(parents=True, exist_ok=True)
     srcs = sources()
@@ -78,6 +107,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stderr}")
     tmp.replace(LIB)
+    build_cli(force=True)
     return LIB
 
 

@@ -550,9 +550,14 @@ struct Engine final : EngineBase {
                                   gate);
     }
 
+    // Limits at the most any instance can ask for, not this engine's current
+    // need: the attribute belongs to the kernel and is shared by every engine
+    // in the process (the same rule as the single-instance solver's).
     cudaError_t set_attributes() {
+        const size_t xlim = pria::Solver<Real>::x_smem_limit();
+        if (x_smem > xlim) return cudaErrorInvalidValue;
         auto xa = [&](auto fn) {
-            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem));
+            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xlim));
         };
         if (tw == 32) {
             RB_CUDA_TRY(xa(bj_x<Real, 32, true, false>));
@@ -563,11 +568,9 @@ struct Engine final : EngineBase {
             RB_CUDA_TRY(xa(bj_x<Real, 16, true, true>));
             RB_CUDA_TRY(xa(bj_x<Real, 16, false, true>));
         }
-        size_t ym = 0;
-        for (int c = 1; c < kMaxGroups; ++c) ym = std::max(ym, yz_smem[c]);
         constexpr int kT = pria::Solver<Real>::kYZThreads;
         auto ya = [&](auto fn) -> cudaError_t {
-            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ym)));
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pria::kSliceBytes));
             return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         };
         RB_CUDA_TRY(ya(bj_yz<Real, kT, true, false>));

@@ -886,6 +886,10 @@ struct Solver final : SolverBase {
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
     static constexpr int kYZThreads = 256;
+    // x tiles: tw columns of a padded row of at most kMaxPeriods (+1) reals
+    static constexpr size_t x_smem_limit() {
+        return size_t(sizeof(Real) == 4 ? 32 : 16) * size_t(kMaxPeriods + 1) * sizeof(Real);
+    }
 
     ~Solver() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -1035,29 +1039,37 @@ struct Solver final : SolverBase {
         return cudaGetLastError();
     }
 
+    // The dynamic shared-memory limit is a property of the kernel, shared by
+    // every solver in the process, so it is set to the most any instance can
+    // ask for (x: a tile of the widest padded row; y/z: one cluster slice),
+    // never to this instance's own need: a later, smaller instance must not
+    // lower the limit under an earlier, larger one.
     template <int TW, bool R, bool C>
     cudaError_t x_attr() {
         return cudaFuncSetAttribute(x_kernel<Real, TW, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(x_smem));
+                                    int(x_smem_limit()));
     }
     template <bool R, bool C>
     cudaError_t yz_attr() {
         auto fn = yz_kernel<Real, kYZThreads, R, C>;
-        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(yz_smem)));
-        if (d.csize > 8) RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
+        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         return cudaSuccess;
     }
     cudaError_t set_attributes() {
+        if (x_smem > x_smem_limit()) return cudaErrorInvalidValue;
         if (tw == 32) {
             RB_CUDA_TRY((x_attr<32, true, false>()));
             RB_CUDA_TRY((x_attr<32, true, true>()));
             RB_CUDA_TRY((x_attr<32, false, true>()));
-            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem)));
+            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(x_smem_limit())));
         } else {
             RB_CUDA_TRY((x_attr<16, true, false>()));
             RB_CUDA_TRY((x_attr<16, true, true>()));
             RB_CUDA_TRY((x_attr<16, false, true>()));
-            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(x_smem)));
+            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(x_smem_limit())));
         }
         RB_CUDA_TRY((yz_attr<true, false>()));
         RB_CUDA_TRY((yz_attr<true, true>()));

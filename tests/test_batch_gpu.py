@@ -129,3 +129,19 @@ def test_autotune_keeps_results(native):
         for i in range(2):
             r = b.result_jrp(2 + i)
             assert r.iterations == sj[i].iterations
+
+
+def test_long_horizon_added_before_short_ones(native):
+    """Instances added largest first: the per-tile shared memory of a long
+    horizon (T = 600, above the 48 KB default) must stay available after
+    shorter instances join; each result still equals its solo run."""
+    from reformulation_b200.batch import Batch
+    js = [jrp_demand(30, 8, 600), jrp_demand(31, 3, 17), jrp_demand(32, 5, 40)]
+    sq, sj = solo([], js, "mixed", 1e-4)
+    with Batch("mixed") as b:
+        ids = [b.add_jrp(j, jp()) for j in js]
+        b.start()
+        b.run()
+        for i, j in zip(ids, sj):
+            r = b.result_jrp(i)
+            assert r.iterations == j.iterations and r.primal_objective == j.primal_objective

@@ -171,3 +171,21 @@ def test_deterministic_and_backend(native):
     assert r.status == "optimal" and r.objective == r.upper and r.entries == inst.entries
     m = pria.solve(inst, tolerances=Tolerances(optimality=1e-4), time_limit=60.0, precision="mixed")
     assert m.status == "optimal" and rel(m.objective, r.objective) <= 1e-3
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_solvers_of_different_sizes_coexist(native, precision):
+    """A long horizon needs more dynamic shared memory per tile than the
+    48 KB default; creating a smaller solver afterwards must not take that
+    away from the larger one (the limit belongs to the kernel, not to a
+    solver).  Both run, and the larger matches a solver created alone."""
+    from reformulation_b200 import pria
+    p = pria.Library().parameters(256, 1e-6)
+    big, small = jrp_demand(30, 8, 600), jrp_demand(31, 3, 17)
+    with pria.DeviceSolver(big, p, precision) as a, pria.DeviceSolver(small, p, precision) as b:
+        assert a.run() == 0 and b.run() == 0
+        ra = a.result()
+    with pria.DeviceSolver(big, p, precision) as c:
+        assert c.run() == 0
+        rc = c.result()
+    assert ra.iterations == rc.iterations and ra.primal_objective == rc.primal_objective
