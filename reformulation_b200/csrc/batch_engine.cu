@@ -360,6 +360,7 @@ struct Engine final : EngineBase {
     int add_jrp(int64_t n, int64_t t, const double* k, double k0, const double* h,
                 const pria_params& p0) override {
         pria_params p = p0;
+        if (!p.use_halpern || p.warm_steps > 0) return -int(cudaErrorNotSupported);   // Halpern blocks only
         if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
         p.op_steps = op_steps;
         std::unique_ptr<pria::SolverBase> base;
@@ -375,6 +376,7 @@ struct Engine final : EngineBase {
     int add_jrp_demand(int64_t n, int64_t t, const double* k, double k0, const double* rate, const double* demand,
                        const pria_params& p0) override {
         pria_params p = p0;
+        if (!p.use_halpern || p.warm_steps > 0) return -int(cudaErrorNotSupported);   // Halpern blocks only
         if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
         p.op_steps = op_steps;
         std::unique_ptr<pria::SolverBase> base;

@@ -71,6 +71,7 @@ struct Control {
     double new_error, lower, upper, gap;
     long long restart_iter, iteration;
     int terminated, restart, result_slot, status;
+    int phase_done;          // the vanilla phase reached its step budget
 };
 
 struct Params {
@@ -79,7 +80,16 @@ struct Params {
     double beta_sufficient, beta_necessary, beta_artificial;
     double theta_target, theta_decay;
     double scale;
+    long long start_max;     // step budget the start check judges against
+    long long vanilla_max;   // step budget of the vanilla phase (< 0: none)
+    double omega0;           // the initial primal weight
+    int vanilla_solve;       // plain PDHG throughout (no Halpern phase)
 };
+
+// Bits of the `gate` argument of the step kernels.
+constexpr int kGateRestart = 1;   // run only when the last check asked for a restart
+constexpr int kGateVanilla = 2;   // vanilla step: next point = the step, anchor untouched
+constexpr int kGateDrift = 4;     // check sums measure the drift from the existing anchor
 
 __host__ __device__ __forceinline__ long long blk(int n, int tp, int s) {
     return (long long)n * ((long long)s * tp - (long long)s * (s - 1) / 2);
@@ -101,7 +111,7 @@ struct Dev {
 };
 
 __device__ __forceinline__ bool skip(const Control* c, int gate) {
-    return c->terminated || (gate && !c->restart);
+    return c->terminated || ((gate & kGateRestart) && !c->restart);
 }
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -259,6 +269,12 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
     __syncthreads();
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    // Without Reflect: a vanilla step (the next point is the step itself and
+    // the anchor stays), or the step that makes the point stepped from the
+    // new anchor (restart; the end of the vanilla phase, whose drift sums are
+    // taken against the old anchor).
+    const bool vanilla = !Reflect && (gate & kGateVanilla);
+    const bool drift = Reflect || (gate & kGateDrift);
     double acc[2] = {0.0, 0.0};
     for (int sb = warp * kRpw + sub; sb < rows; sb += rstep * kUnroll) {
         long long ev[kUnroll];
@@ -270,7 +286,7 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
             if (s < rows && col < tcols && tt >= s) {
                 ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
                 x1v[u] = xsrc[ev[u]];
-                xav[u] = Reflect ? d.x0[ev[u]] : x1v[u];
+                xav[u] = drift ? d.x0[ev[u]] : x1v[u];
             }
         }
 #pragma unroll
@@ -278,14 +294,14 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
             if (ev[u] < 0) continue;
             const long long e = ev[u];
             const Real x2 = Real(fmax(double(pre[col * stride + sb + u * rstep]) - theta[col], 0.0));
-            const Real x1 = x1v[u], xa = xav[u];
+            const Real x1 = x1v[u], xa = Reflect ? xav[u] : x1;
             d.r[e] = sigma * (Real(2) * x2 - x1);
-            d.xh[e] = lwn * (Real(2) * x2 - x1) + rwn * xa;
-            if (!Reflect) d.x0[e] = x1;
+            d.xh[e] = vanilla ? x2 : lwn * (Real(2) * x2 - x1) + rwn * xa;
+            if (!Reflect && !vanilla) d.x0[e] = x1;
             if (Check) {
                 d.x2s[e] = x2;
                 d.dxs[e] = x1 - x2;
-                const double dx = double(x1) - double(x2), dr = double(x1) - double(xa);
+                const double dx = double(x1) - double(x2), dr = double(x1) - double(xav[u]);
                 acc[0] += dx * dx;
                 acc[1] += dr * dr;
             }
@@ -326,6 +342,8 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads / 32;
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    const bool vanilla = !Reflect && (gate & kGateVanilla);   // as in the x half-step
+    const bool drift = Reflect || (gate & kGateDrift);
     double acc[3] = {0.0, 0.0, 0.0};   // |dy|^2 + |dz|^2, <dx, dy + dz>, drift
 
     // phase A: y rows, and the z values into shared memory
@@ -351,12 +369,13 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
                 const long long e = e0 + q;
                 const Real y2 = Real(fmax(double(v[k]) - th, 0.0));
                 const Real y1 = ysrc[e];
-                const Real ya = Reflect ? d.y0[e] : y1;
-                d.yh[e] = lwn * (Real(2) * y2 - y1) + rwn * ya;
-                if (!Reflect) d.y0[e] = y1;
+                const Real yd = drift ? d.y0[e] : y1;
+                const Real ya = Reflect ? yd : y1;
+                d.yh[e] = vanilla ? y2 : lwn * (Real(2) * y2 - y1) + rwn * ya;
+                if (!Reflect && !vanilla) d.y0[e] = y1;
                 if (Check) {
                     if (Reflect) d.y2s[e] = y2;
-                    const double dy = double(y1) - double(y2), dr = double(y1) - double(ya);
+                    const double dy = double(y1) - double(y2), dr = double(y1) - double(yd);
                     acc[0] += dy * dy;
                     acc[1] += double(d.dxs[e]) * dy;
                     acc[2] += dr * dr;
@@ -411,7 +430,7 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
             const int q = qb + u * kThreads;
             if (q < mine) {
                 z1v[u] = zsrc[sbase + q];
-                zav[u] = Reflect ? d.z0[sbase + q] : z1v[u];
+                zav[u] = drift ? d.z0[sbase + q] : z1v[u];
                 if (Check) dxv[u] = d.dxs[sbase + q];
             }
         }
@@ -421,12 +440,12 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
             if (q >= mine) continue;
             const long long e = sbase + q;
             const Real z2 = Real(fmax(double(vz[q]) - thz, 0.0));
-            const Real z1 = z1v[u], za = zav[u];
-            d.zh[e] = lwn * (Real(2) * z2 - z1) + rwn * za;
-            if (!Reflect) d.z0[e] = z1;
+            const Real z1 = z1v[u], za = Reflect ? zav[u] : z1;
+            d.zh[e] = vanilla ? z2 : lwn * (Real(2) * z2 - z1) + rwn * za;
+            if (!Reflect && !vanilla) d.z0[e] = z1;
             if (Check) {
                 if (Reflect) d.z2s[e] = z2;
-                const double dz = double(z1) - double(z2), dr = double(z1) - double(za);
+                const double dz = double(z1) - double(z2), dr = double(z1) - double(zav[u]);
                 acc[0] += dz * dz;
                 acc[1] += double(dxv[u]) * dz;
                 acc[2] += dr * dr;
@@ -550,7 +569,10 @@ __device__ __forceinline__ bool should_stop(double gap, long long iteration, con
 }
 
 // mode 0: the check before the loop; 1: after an op_steps block; 2: after the
-// restart step (solver.py:514-594).
+// restart step (solver.py:514-594); 3: after a block of vanilla steps (the
+// bounds at the current point, solver.py:601-606); 4: after the step that
+// ends the vanilla phase and starts the Halpern one (the primal weight from
+// the drift of the vanilla phase, solver.py:680-694).
 __device__ __forceinline__ void check_body(Control* c, Params p, const double* __restrict__ px, int nbx,
              const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
              const double* __restrict__ plo, int nblo, int mode) {
@@ -558,13 +580,48 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* _
     if (mode == 2 && !c->restart) return;
     __shared__ double scratch[3 * 32];
     __shared__ double xs[2], yzs[3], up[3], lo[1];
-    reduce_rows<2>(px, nbx, scratch, xs);
-    reduce_rows<3>(pyz, nbyz, scratch, yzs);
-    if (mode != 2) {
+    if (mode != 3) {
+        reduce_rows<2>(px, nbx, scratch, xs);
+        reduce_rows<3>(pyz, nbyz, scratch, yzs);
+    }
+    if (mode != 2 && mode != 4) {
         reduce_rows<3>(pup, nbup, scratch, up);
         reduce_rows<1>(plo, nblo, scratch, lo);
     }
     if (threadIdx.x != 0) return;
+    if (mode == 4) {
+        // omega = |d(y, z)| / |dx| over the vanilla phase, NaN -> the initial one
+        if (c->iteration > 0) {
+            const double om = sqrt(yzs[2]) / sqrt(xs[1]);
+            c->omega = isnan(om) ? p.omega0 : om;
+        }
+        c->fp_error = canonical(xs, yzs, c->omega, p.eta);
+        c->new_error = c->fp_error;
+        c->check_error = INFINITY;
+        c->restart_iter = 0;
+        c->restart = 0;
+        c->phase_done = 0;
+        c->result_slot = 1;   // the point the gap was measured at is now the anchor
+        c->terminated = should_stop(c->gap, c->iteration, p) ? 1 : 0;
+        return;
+    }
+    if (mode == 3) {
+        const double upper = (up[0] + up[1] + up[2]) * p.scale;
+        const double lower = lo[0] * p.scale;
+        const double gap = (upper - lower) / (1.0 + fabs(lower) + fabs(upper));
+        c->upper = upper;
+        c->lower = lower;
+        c->gap = gap;
+        c->iteration += p.op_steps;
+        c->result_slot = 3;
+        const bool within = c->iteration < p.vanilla_max || p.vanilla_max < 0;
+        if (!(gap > p.tolerance)) c->terminated = 1;
+        else if (!within) {
+            if (p.vanilla_solve) c->terminated = 1;   // a vanilla solve: its iteration limit
+            else c->phase_done = 1;
+        }
+        return;
+    }
     if (mode == 2) {
         c->fp_error = canonical(xs, yzs, c->omega, p.eta);
         c->check_error = INFINITY;
@@ -582,7 +639,9 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* _
         c->fp_error = canonical(xs, yzs, c->omega, p.eta);
         c->new_error = c->fp_error;
         c->check_error = INFINITY;
-        c->terminated = should_stop(gap, c->iteration, p) ? 1 : 0;
+        Params q = p;
+        q.max_iter = p.start_max;
+        c->terminated = should_stop(gap, c->iteration, q) ? 1 : 0;
         c->result_slot = 1;
         c->restart = 0;
         return;
@@ -652,6 +711,7 @@ __global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta)
         c->restart = 0;
         c->result_slot = 1;
         c->status = 0;
+        c->phase_done = 0;
     }
 }
 
@@ -1034,6 +1094,10 @@ struct Solver final : SolverBase {
         prm.beta_artificial = p.beta_artificial;
         prm.theta_target = p.theta_target;
         prm.theta_decay = p.theta_decay;
+        prm.vanilla_max = p.use_halpern ? (long long)p.op_steps * p.warm_steps : p.max_iter;
+        prm.start_max = vanilla_phase() ? prm.vanilla_max : p.max_iter;
+        prm.omega0 = p.omega;
+        prm.vanilla_solve = p.use_halpern ? 0 : 1;
         RB_CUDA_TRY(set_attributes());
         block_nodes = 2LL * p.op_steps + 3 + 3;
         return cudaGetLastError();
@@ -1074,8 +1138,16 @@ struct Solver final : SolverBase {
         RB_CUDA_TRY((yz_attr<true, false>()));
         RB_CUDA_TRY((yz_attr<true, true>()));
         RB_CUDA_TRY((yz_attr<false, true>()));
+        if (vanilla_phase()) {
+            RB_CUDA_TRY(tw == 32 ? (x_attr<32, false, false>()) : (x_attr<16, false, false>()));
+            RB_CUDA_TRY((yz_attr<false, false>()));
+        }
         return cudaSuccess;
     }
+
+    // Plain PDHG: the whole solve without Halpern, or warm_steps check blocks
+    // before it (solver.py:601-606, 680-694).
+    bool vanilla_phase() const { return !p.use_halpern || p.warm_steps > 0; }
 
     template <bool R, bool C>
     cudaError_t launch_x(const Real* xs, const Real* ys, const Real* zs, int step, int gate) {
@@ -1212,10 +1284,50 @@ struct Solver final : SolverBase {
         return cudaStreamSynchronize(stream);
     }
 
+    // One check block of the vanilla phase: op_steps plain steps of the
+    // current point in place, then the bounds at it and the check (mode 3).
+    cudaError_t enqueue_vanilla_block() {
+        for (int s = 0; s < p.op_steps; ++s) {
+            RB_CUDA_TRY((launch_x<false, false>(d.xh, d.yh, d.zh, 0, kGateVanilla)));
+            RB_CUDA_TRY((launch_yz<false, false>(d.yh, d.zh, 0, kGateVanilla)));
+        }
+        upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.xh, tp, 0);
+        lower_kernel<Real><<<nblo, kAuxThreads, 0, stream>>>(d, d.yh, d.zh);
+        RB_CUDA_TRY(launch_check(3));
+        nlaunch += 2LL * p.op_steps + 3;
+        return cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+    }
+
+    // The vanilla phase from the start point (x0, the anchor, is kept for
+    // the drift that sets omega), then, for the Halpern method, the step
+    // that makes the current point the anchor (mode 4).
+    cudaError_t run_vanilla() {
+        const size_t bytes = sizeof(Real) * size_t(nd);
+        RB_CUDA_TRY(cudaMemcpyAsync(d.xh, d.x0, bytes, cudaMemcpyDeviceToDevice, stream));
+        RB_CUDA_TRY(cudaMemcpyAsync(d.yh, d.y0, bytes, cudaMemcpyDeviceToDevice, stream));
+        RB_CUDA_TRY(cudaMemcpyAsync(d.zh, d.z0, bytes, cudaMemcpyDeviceToDevice, stream));
+        for (;;) {
+            RB_CUDA_TRY(enqueue_vanilla_block());
+            RB_CUDA_TRY(cudaStreamSynchronize(stream));
+            if (mirror->terminated || mirror->phase_done) break;
+            if (p.verbose)
+                fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  (vanilla)\n",
+                        mirror->iteration, mirror->upper, mirror->lower, mirror->gap);
+        }
+        if (mirror->terminated || !p.use_halpern) return cudaSuccess;
+        RB_CUDA_TRY((launch_x<false, true>(d.xh, d.yh, d.zh, 0, kGateDrift)));
+        RB_CUDA_TRY((launch_yz<false, true>(d.yh, d.zh, 0, kGateDrift)));
+        RB_CUDA_TRY(launch_check(4));
+        nlaunch += 3;
+        RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+        return cudaStreamSynchronize(stream);
+    }
+
     int run() override {
-        if (runs++ > 0 && !exec && capture_block() != cudaSuccess) return int(cudaErrorUnknown);
+        if (runs++ > 0 && !exec && p.use_halpern && capture_block() != cudaSuccess) return int(cudaErrorUnknown);
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
+        if (!mirror->terminated && vanilla_phase() && (st = run_vanilla()) != cudaSuccess) return int(st);
         if (!mirror->terminated) {
             for (int kk = 0; kk < 2; ++kk) {
                 if ((st = launch_block()) != cudaSuccess) return int(st);
@@ -1245,6 +1357,8 @@ struct Solver final : SolverBase {
         for (int kk = 0; kk < kKinds; ++kk) { ms[kk] = 0.0; count[kk] = 0; }
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
+        // the vanilla phase, if any, runs untimed: the kinds are the Halpern block's
+        if (!mirror->terminated && vanilla_phase() && (st = run_vanilla()) != cudaSuccess) return int(st);
         profiling = true;
         while (!mirror->terminated) {
             marks.clear();
@@ -1272,7 +1386,7 @@ struct Solver final : SolverBase {
 
     // The objective at the returned (unpadded) x, in instance units.
     cudaError_t final_primal(double* out) {
-        const Real* xs = mirror->result_slot == 1 ? d.x0 : d.x2s;
+        const Real* xs = point(0);
         Dev<Real> dd = d;
         dd.pup = final_up.ptr;
         upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(dd, xs, t, 1);
@@ -1296,12 +1410,22 @@ struct Solver final : SolverBase {
         return cudaStreamSynchronize(stream);
     }
 
+    // The returned point: 1 the anchor (the start, or the point the vanilla
+    // phase ended at), 2 the step at the last check, 3 the current point of
+    // a vanilla solve.  k = 0, 1, 2 for x, y, z.
+    const Real* point(int k) const {
+        const int slot = mirror->result_slot;
+        const Real* const anchor[3] = {d.x0, d.y0, d.z0};
+        const Real* const step[3] = {d.x2s, d.y2s, d.z2s};
+        const Real* const cur[3] = {d.xh, d.yh, d.zh};
+        return slot == 1 ? anchor[k] : slot == 3 ? cur[k] : step[k];
+    }
+
     template <class Out>
     int result_t(Out* x, Out* y, Out* z, pria_result_info* info) {
-        const bool start = mirror->result_slot == 1;
-        const Real* xs = start ? d.x0 : d.x2s;
-        const Real* ys = start ? d.y0 : d.y2s;
-        const Real* zs = start ? d.z0 : d.z2s;
+        const Real* xs = point(0);
+        const Real* ys = point(1);
+        const Real* zs = point(2);
         cudaError_t st;
         if (x && (st = unpack<Out>(xs, 0, x)) != cudaSuccess) return int(st);
         if (y && (st = unpack<Out>(ys, 1, y)) != cudaSuccess) return int(st);
@@ -1343,11 +1467,6 @@ static int create(int64_t n, int64_t t, const In* K, double K0, const In* H, con
     pria_params p = *params;
     if (p.op_steps < 2) p.op_steps = 2;
     if (p.warm_steps < 0) p.warm_steps = 0;
-    if (!p.use_halpern || p.warm_steps > 0) {
-        // the vanilla loop (and the warm phase) of solver.py:601-606 is not
-        // built: only the restarted Halpern method with warm_steps = 0
-        return int(cudaErrorNotSupported);
-    }
     if (p.max_iter < 0) p.max_iter = -1;
     cudaError_t st;
     if (use_float32) {
@@ -1372,7 +1491,7 @@ static int create_demand(int64_t n, int64_t t, const double* K, double K0, const
     if (tp > kMaxPeriods || n > (1LL << 24)) return int(cudaErrorInvalidValue);
     pria_params p = *params;
     if (p.op_steps < 2) p.op_steps = 2;
-    if (!p.use_halpern || p.warm_steps > 0) return int(cudaErrorNotSupported);
+    if (p.warm_steps < 0) p.warm_steps = 0;
     if (p.max_iter < 0) p.max_iter = -1;
     cudaError_t st;
     if (use_float32) {

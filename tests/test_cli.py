@@ -175,3 +175,18 @@ def test_pria_cli_equals_library(bins, tmp_path, f32):
     r = run(bins[1], tmp_path / "j.bin", tmp_path / "r2.bin", str(tol), "-1", *(["f32"] if f32 else []))
     assert r.returncode == 0
     assert read_pria(tmp_path / "r2.bin")["iterations"] == out["iterations"]
+
+
+@pytest.mark.gpu
+def test_pria_cli_vanilla_and_verbose(bins, tmp_path):
+    from reformulation_b200 import pria
+    j = jrp_demand(8, 5, 14)
+    write_pria(j, tmp_path / "j.bin")
+    r = run(bins[1], tmp_path / "j.bin", tmp_path / "r.bin", "1e-12", "64", "vanilla", "verbose")
+    assert r.returncode == 1, r.stderr          # the cap, not the gap, ended it
+    out = read_pria(tmp_path / "r.bin")
+    lib = pria.Library()
+    s = lib.solve(j, lib.parameters(64, 1e-12, use_halpern=0))
+    assert out["iterations"] == s.iterations == 64 and out["status"] == 1
+    assert out["upper"] == s.primal_objective and out["lower"] == s.dual_objective
+    assert "vanilla" in r.stderr                # per-check progress lines

@@ -89,6 +89,26 @@ def test_pria_oracle_matches_reference_live(oracle_lib):
     assert rel(a["lower"], b["lower"]) <= 1e-9
 
 
+PRIA_PLAIN_MODES = [dict(use_halpern=0, max_iter=96, tolerance=1e-12),
+                    dict(use_halpern=0, max_iter=-1, tolerance=1e-6),
+                    dict(warm_steps=3, tolerance=1e-6), dict(warm_steps=2, max_iter=16, tolerance=1e-12)]
+PRIA_PLAIN_IDS = ["vanilla-cap", "vanilla-tol", "warm3", "warm-past-cap"]
+
+
+@pytest.mark.parametrize("mode", PRIA_PLAIN_MODES, ids=PRIA_PLAIN_IDS)
+def test_pria_oracle_vanilla_and_warm_phase_match_reference(oracle_lib, mode):
+    """Plain PDHG (use_halpern = 0) and the vanilla warm phase before Halpern
+    (warm_steps > 0) of jrp/pria-cuda/tests/ref_impl.hpp:297-330."""
+    if not oracle_lib.ref_pria_available():
+        pytest.skip("oracle/_ref not built")
+    inst = oracle_lib.ref_pria_random_instance(17, 5, 12)
+    p = oracle_lib.pria_params(**mode)
+    a = oracle_lib.pria_solve(inst, p)
+    b = oracle_lib.ref_pria_solve(inst, p)
+    assert a["iterations"] == b["iterations"]
+    assert rel(a["lower"], b["lower"]) <= 1e-9 and rel(a["upper"], b["upper"]) <= 1e-9
+
+
 def test_maxflow_matches_enumeration(oracle_lib):
     rng = np.random.default_rng(5)
     for k in range(20):

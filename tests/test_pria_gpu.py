@@ -189,3 +189,36 @@ def test_solvers_of_different_sizes_coexist(native, precision):
         assert c.run() == 0
         rc = c.result()
     assert ra.iterations == rc.iterations and ra.primal_objective == rc.primal_objective
+
+
+PLAIN_MODES = [dict(use_halpern=0, max_iter=96, tolerance=1e-12),
+               dict(use_halpern=0, max_iter=-1, tolerance=1e-6),
+               dict(warm_steps=3, tolerance=1e-6), dict(warm_steps=2, max_iter=16, tolerance=1e-12)]
+
+
+@pytest.mark.parametrize("mode", PLAIN_MODES, ids=["vanilla-cap", "vanilla-tol", "warm3", "warm-past-cap"])
+def test_vanilla_and_warm_phase_match_reference(lib, oracle_lib, mode):
+    """Plain PDHG (use_halpern = 0, the CLI's `vanilla` flag) and warm_steps
+    vanilla blocks before the Halpern method, against the reference's own CPU
+    solver (jrp/pria-cuda/tests/ref_impl.hpp:297-330): the same iteration
+    count (a cap is exact; the warm phase may run past max_iter, as the
+    reference's does), bounds within 1e-6 relative."""
+    inst = oracle_lib.ref_pria_random_instance(17, 5, 12)
+    ref = oracle_lib.ref_pria_solve(inst, oracle_lib.pria_params(**mode))
+    p = lib.parameters(mode.get("max_iter", -1), mode["tolerance"],
+                       **{k: v for k, v in mode.items() if k not in ("max_iter", "tolerance")})
+    s = lib.solve(inst, p, want_solution=True)
+    assert s.status == 0
+    if mode["tolerance"] < 1e-10:
+        assert s.iterations == ref["iterations"]
+    else:
+        assert abs(s.iterations - ref["iterations"]) <= 16 and s.relative_gap <= mode["tolerance"]
+    assert rel(s.dual_objective, ref["lower"]) <= 1e-6
+    assert rel(s.primal_objective, ref["upper"]) <= 1e-6
+    feasible(inst, s)
+    # FP32 iterates: a 1e-4 gap, with a cap (they level off near 1e-6)
+    cap = mode.get("max_iter", -1)
+    pm = lib.parameters(cap if cap > 0 else 5000, max(mode["tolerance"], 1e-4),
+                        **{k: v for k, v in mode.items() if k not in ("max_iter", "tolerance")})
+    m = lib.solve(inst, pm, precision="mixed")
+    assert m.status == 0 and rel(m.primal_objective, s.primal_objective) <= 1e-3
