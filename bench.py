@@ -459,7 +459,7 @@ def run_batch(args):
     import torch
 
     from reformulation_b200 import praq, pria
-    from reformulation_b200.batch import Batch
+    from reformulation_b200.batch import EscalatingBatch
     from reformulation_b200.instances import batch_mix
 
     torch.cuda.set_device(0)
@@ -470,12 +470,12 @@ def run_batch(args):
     ql, jl = praq.Library(), pria.Library()
     qp = ql.parameters(tolerance=TOL, max_iter=1_000_000, use_float32=1)
     jp = jl.parameters(1_000_000, TOL)
-    b = Batch("mixed", stream=stream.cuda_stream)
+    b = EscalatingBatch(stream=stream.cuda_stream)
     t_lay = time.perf_counter()
     ids = [b.add_qubo(q, qp) for q in qs] + [b.add_jrp_demand(j, jp) for j in js]
     b.start()
     t_lay = time.perf_counter() - t_lay
-    shapes = b.autotune() if args.autotune else None
+    shapes = b.b32.autotune() if args.autotune else None
     for _ in range(args.warmup):
         b.restart()
         b.run()
@@ -522,6 +522,7 @@ def run_batch(args):
             "ms_per_step": sum(ms) / len(ms), "dtype": "f32 iterates, f64 reductions",
             "instances": total, "max_gap": max(gaps), "iterations_p50": float(np.percentile(its, 50)),
             "iterations_max": int(max(its)), "device_bytes": b.device_bytes(), "shapes": shapes,
+            "escalated_to_fp64": len(b.escalated),
             "gpu_launches": int(launches),
             "plain_fp64_sequential": {"value": fp64_value, "unit": UNIT, "sample": len(sample),
                                       "sample_stride": args.fp64_stride},

@@ -107,6 +107,15 @@ REFORM_API int reform_praq_run(reform_praq_solver* solver);
  * (y2 [2m], may be NULL) and result. */
 REFORM_API int reform_praq_result(reform_praq_solver* solver, double* x, double* y2, PraqResult* result);
 
+/* A warm start for the following runs, as the reference's
+ * solve_qubo_problem_warm_start (qubo/praq-jax/praq/solver.py:482-560): x [n]
+ * and dual pairs y2 [2m] in instance units and the instance's own edge order
+ * (what reform_praq_result returns); both are projected (x clipped to [0, 1],
+ * each pair onto its edge's dual set), so any point may be given.  Either may
+ * be NULL (x = 1/2, or the centroid of the dual set); both NULL restores the
+ * cold start.  The arrays are copied; the call returns when they are. */
+REFORM_API int reform_praq_set_warm(reform_praq_solver* solver, const double* x, const double* y2);
+
 /* A wall-clock budget for each run, in seconds (< 0: none, the default).
  * When it runs out the run stops between two checks and returns
  * PRAQ_STATUS_TIME_LIMIT; the result is the bracket of the last completed

@@ -40,7 +40,7 @@ typedef struct reform_batch reform_batch;
 
 /* Tunable launch shapes (reform_batch_autotune picks them; zero = default). */
 typedef struct {
-    int praq_half_edges_per_lane;  /* node-kernel lanes per node target: 2, 4 or 8 */
+    int reserved0;                 /* unused, 0 */
     int grid_multiplier;           /* persistent CTAs per SM for the step kernels: 2..16 */
     int reserved[6];
 } reform_shapes;
@@ -92,8 +92,18 @@ REFORM_API int reform_batch_result_qubo(reform_batch* b, int id, double* x, Praq
 REFORM_API int reform_batch_result_jrp(reform_batch* b, int id, double* x, double* y, double* z,
                                        pria_result_info* info);
 
-/* Free an instance's device memory (it must be done or never started). */
+/* Free an instance's device memory.  A running instance first leaves the
+ * schedule (after the blocks in flight have finished). */
 REFORM_API int reform_batch_remove(reform_batch* b, int id);
+
+/* QUBO warm start of an instance added and not yet started (as
+ * reform_praq_set_warm: x [n], dual pairs y2 [2m], instance units, projected). */
+REFORM_API int reform_batch_set_warm_qubo(reform_batch* b, int id, const double* x, const double* y2);
+
+/* The point of a started QUBO instance's last check (x [n], dual pairs y2
+ * [2m], instance units; either may be NULL), running or done: what a warm
+ * start elsewhere continues from. */
+REFORM_API int reform_batch_point_qubo(reform_batch* b, int id, double* x, double* y2);
 
 /* Device bytes held by the instances of the batch (their layouts and iterates). */
 REFORM_API int64_t reform_batch_device_bytes(const reform_batch* b);

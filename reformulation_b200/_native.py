@@ -56,7 +56,7 @@ class PriaResultInfo(ctypes.Structure):
 
 
 class ReformShapes(ctypes.Structure):
-    _fields_ = [("praq_half_edges_per_lane", c_int), ("grid_multiplier", c_int),
+    _fields_ = [("reserved0", c_int), ("grid_multiplier", c_int),
                 ("reserved", c_int * 6)]
 
 
@@ -75,6 +75,7 @@ def _declare(lib):
         "reform_praq_run": (I, [c_void_p]),
         "reform_praq_result": (I, [c_void_p, D, D, P(PraqResult)]),
         "reform_praq_set_time_limit": (I, [c_void_p, c_double]),
+        "reform_praq_set_warm": (I, [c_void_p, P(c_double), P(c_double)]),
         "reform_praq_run_profiled": (I, [c_void_p, D, P(c_int64)]),
         "reform_praq_launches": (c_int64, [c_void_p]),
         "reform_praq_destroy": (None, [c_void_p]),
@@ -117,6 +118,8 @@ def _declare(lib):
         "reform_batch_result_qubo": (I, [V, I, D, P(PraqResult)]),
         "reform_batch_result_jrp": (I, [V, I, D, D, D, P(PriaResultInfo)]),
         "reform_batch_remove": (I, [V, I]),
+        "reform_batch_set_warm_qubo": (I, [V, I, D, D]),
+        "reform_batch_point_qubo": (I, [V, I, D, D]),
         "reform_batch_device_bytes": (c_int64, [V]),
         "reform_batch_set_shapes": (I, [V, P(ReformShapes)]),
         "reform_batch_autotune": (I, [V, P(ReformShapes)]),

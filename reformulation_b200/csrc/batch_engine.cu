@@ -217,7 +217,6 @@ struct Table {
 };
 
 struct Shapes {
-    double praq_per_lane = 4.0;
     int grid_mult = 8;
 };
 
@@ -238,6 +237,8 @@ struct EngineBase {
     virtual int inflight() const = 0;
     virtual int status(int id, int* done, int64_t* it, double* lo, double* up) = 0;
     virtual int result_qubo(int id, double* x, PraqResult* r) = 0;
+    virtual int set_warm_qubo(int id, const double* x, const double* y2) = 0;
+    virtual int point_qubo(int id, double* x, double* y2) = 0;
     virtual int result_jrp(int id, double* x, double* y, double* z, pria_result_info* info) = 0;
     virtual int remove(int id) = 0;
     virtual int64_t device_bytes() const = 0;
@@ -290,7 +291,7 @@ struct Engine final : EngineBase {
 
     size_t x_smem = 0, yz_smem[kMaxGroups] = {};
     bool groups[kMaxGroups] = {};
-    int tw = sizeof(Real) == 4 ? 32 : 16;
+    static constexpr int tw = pria::kXTile;
     bool dirty = true;          // the graph must be captured again
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -350,7 +351,6 @@ struct Engine final : EngineBase {
         s->p = p;
         const int st = s->setup(in, stream);
         if (st) return st;
-        s->set_lanes_target(shapes.praq_per_lane);
         q.push_back(QInst{std::move(s)});
         ids.emplace_back(0, int(q.size()) - 1);
         dirty = true;
@@ -521,12 +521,8 @@ struct Engine final : EngineBase {
     template <bool R, bool C>
     cudaError_t launch_x(int step, int gate) {
         const int grid = std::max(1, sms * std::max(1, int((228 * 1024) / std::max<size_t>(x_smem + 2048, 1))));
-        if (tw == 32)
-            bj_x<Real, 32, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
-                                                                        counts.ptr + kX, step, gate);
-        else
-            bj_x<Real, 16, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
-                                                                        counts.ptr + kX, step, gate);
+        bj_x<Real, tw, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
+                                                                     counts.ptr + kX, step, gate);
         return cudaGetLastError();
     }
 
@@ -561,15 +557,9 @@ struct Engine final : EngineBase {
         auto xa = [&](auto fn) {
             return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xlim));
         };
-        if (tw == 32) {
-            RB_CUDA_TRY(xa(bj_x<Real, 32, true, false>));
-            RB_CUDA_TRY(xa(bj_x<Real, 32, true, true>));
-            RB_CUDA_TRY(xa(bj_x<Real, 32, false, true>));
-        } else {
-            RB_CUDA_TRY(xa(bj_x<Real, 16, true, false>));
-            RB_CUDA_TRY(xa(bj_x<Real, 16, true, true>));
-            RB_CUDA_TRY(xa(bj_x<Real, 16, false, true>));
-        }
+        RB_CUDA_TRY(xa(bj_x<Real, tw, true, false>));
+        RB_CUDA_TRY(xa(bj_x<Real, tw, true, true>));
+        RB_CUDA_TRY(xa(bj_x<Real, tw, false, true>));
         constexpr int kT = pria::Solver<Real>::kYZThreads;
         auto ya = [&](auto fn) -> cudaError_t {
             RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pria::kSliceBytes));
@@ -791,6 +781,26 @@ struct Engine final : EngineBase {
         return qi.s->result(x, nullptr, r);
     }
 
+    int set_warm_qubo(int id, const double* x, const double* y2) override {
+        if (id < 0 || id >= int(ids.size()) || ids[id].first != 0) return PRAQ_ERROR_ARGUMENT;
+        auto& qi = q[ids[id].second];
+        if (!qi.s || qi.started) return PRAQ_ERROR_ARGUMENT;
+        return qi.s->set_warm(x, y2);
+    }
+
+    // The point of the instance's last check (its bracket's primal and dual),
+    // in instance units, whether or not it has terminated.
+    int point_qubo(int id, double* x, double* y2) override {
+        if (id < 0 || id >= int(ids.size()) || ids[id].first != 0) return PRAQ_ERROR_ARGUMENT;
+        auto& qi = q[ids[id].second];
+        if (!qi.s || !qi.started) return PRAQ_ERROR_ARGUMENT;
+        if (pending && drain()) return PRAQ_ERROR_CUDA;
+        if (cudaMemcpyAsync(qi.s->mirror, qi.s->d.ctl, sizeof(praq::Control), cudaMemcpyDeviceToHost, stream) ||
+            cudaStreamSynchronize(stream))
+            return PRAQ_ERROR_CUDA;
+        return qi.s->result(x, y2, nullptr);
+    }
+
     int result_jrp(int id, double* x, double* y, double* z, pria_result_info* info) override {
         if (id < 0 || id >= int(ids.size()) || ids[id].first != 1) return int(cudaErrorInvalidValue);
         auto& ji = j[ids[id].second];
@@ -802,15 +812,16 @@ struct Engine final : EngineBase {
         return ji.s->result(x, y, z, info);
     }
 
+    // A running instance leaves the work tables first (after the blocks in
+    // flight have finished); then its device memory is freed.
     int remove(int id) override {
         if (id < 0 || id >= int(ids.size())) return PRAQ_ERROR_ARGUMENT;
         const auto [kind, k] = ids[id];
         const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
                                        : (j[k].s && j[k].started && !j[k].done);
-        if (running) return PRAQ_ERROR_ARGUMENT;
         if (pending && drain()) return PRAQ_ERROR_CUDA;
         if (kind == 0) q[k].s.reset(); else j[k].s.reset();
-        return 0;
+        return running ? rebuild() : 0;
     }
 
     int64_t device_bytes() const override {
@@ -822,15 +833,12 @@ struct Engine final : EngineBase {
 
     int apply_shapes(const Shapes& sh) {
         shapes = sh;
-        for (auto& qi : q)
-            if (qi.s && qi.s->set_lanes_target(sh.praq_per_lane)) return PRAQ_ERROR_CUDA;
         dirty = true;
         return 0;
     }
 
     int set_shapes(const reform_shapes& s) override {
         Shapes sh = shapes;
-        if (s.praq_half_edges_per_lane > 0) sh.praq_per_lane = s.praq_half_edges_per_lane;
         if (s.grid_multiplier > 0) sh.grid_mult = std::min(16, std::max(1, s.grid_multiplier));
         shapes_fixed = true;
         if (pending && drain()) return PRAQ_ERROR_CUDA;
@@ -866,20 +874,12 @@ struct Engine final : EngineBase {
             auto it = tuned.find(key);
             if (it != tuned.end()) {
                 const int rc = apply_shapes(it->second);
-                if (!rc && out) {
-                    out->praq_half_edges_per_lane = int(it->second.praq_per_lane);
-                    out->grid_multiplier = it->second.grid_mult;
-                }
+                if (!rc && out) out->grid_multiplier = it->second.grid_mult;
                 return rc ? rc : restart_all();
             }
         }
         std::vector<Shapes> cands;
-        for (double pl : {2.0, 4.0, 8.0})
-            for (int gm : {2, 4, 8, 16}) cands.push_back(Shapes{pl, gm});
-        if (q.empty()) {
-            cands.clear();
-            for (int gm : {2, 4, 8, 16}) cands.push_back(Shapes{4.0, gm});
-        }
+        for (int gm : {2, 4, 8, 16}) cands.push_back(Shapes{gm});
         cudaEvent_t a, b;
         if (cudaEventCreate(&a) || cudaEventCreate(&b)) return -1;
         float best = 1e30f;
@@ -906,10 +906,7 @@ struct Engine final : EngineBase {
             std::lock_guard<std::mutex> lock(tuned_mu);
             tuned[key] = pick;
         }
-        if (out) {
-            out->praq_half_edges_per_lane = int(pick.praq_per_lane);
-            out->grid_multiplier = pick.grid_mult;
-        }
+        if (out) out->grid_multiplier = pick.grid_mult;
         if (apply_shapes(pick)) return -1;
         return restart_all();
     }
@@ -987,6 +984,12 @@ int reform_batch_result_jrp(reform_batch* b, int id, double* x, double* y, doubl
     return b ? b->impl->result_jrp(id, x, y, z, info) : PRAQ_ERROR_ARGUMENT;
 }
 int reform_batch_remove(reform_batch* b, int id) { return b ? b->impl->remove(id) : PRAQ_ERROR_ARGUMENT; }
+int reform_batch_set_warm_qubo(reform_batch* b, int id, const double* x, const double* y2) {
+    return b ? b->impl->set_warm_qubo(id, x, y2) : PRAQ_ERROR_ARGUMENT;
+}
+int reform_batch_point_qubo(reform_batch* b, int id, double* x, double* y2) {
+    return b ? b->impl->point_qubo(id, x, y2) : PRAQ_ERROR_ARGUMENT;
+}
 int64_t reform_batch_device_bytes(const reform_batch* b) { return b ? b->impl->device_bytes() : 0; }
 int reform_batch_set_shapes(reform_batch* b, const reform_shapes* s) {
     return b && s ? b->impl->set_shapes(*s) : PRAQ_ERROR_ARGUMENT;

@@ -58,7 +58,10 @@ namespace {
 
 constexpr double kEta = 0.999;   // 0.999 / ||A||_2, ||A||_2 = 1 for the half-edge lift
 constexpr int kBlock = 256;
-constexpr int kEdgesPerThread = 4;
+#ifndef RB200_PRAQ_EDGES_PER_THREAD
+#define RB200_PRAQ_EDGES_PER_THREAD 4   // compile-time tunable (sweeps build with -D)
+#endif
+constexpr int kEdgesPerThread = RB200_PRAQ_EDGES_PER_THREAD;
 constexpr int kNodeSums = 3;     // sum deg (x1-x2)^2, sum deg (x1-x0)^2, sum d . bx
 constexpr int kEdgeSums = 5;     // sum |y1-y2|^2, <S(x1-x2), y1-y2>, sum |y1-y0|^2,
                                  // upper edge term at bx, sum of covering by_1
@@ -87,7 +90,7 @@ struct Params {
 
 template <class Real>
 struct Dev {
-    int n, m, lanes, lane_shift;
+    int n, m;
     const int* row_ptr;    // [n+1] first-end runs in sorted edge order
     const int* col_ptr;    // [n+1] second-end runs in second-end order
     const int* colpos;     // [m] position of sorted edge s in second-end order
@@ -108,30 +111,51 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
     return c->terminated || (gate && !c->restart);
 }
 
-// S^T y at node i, summed over a group of `lanes` lanes (every lane ends with
-// the same bits): the run [row_ptr[i], row_ptr[i+1]) of `ys` plus the run
-// [col_ptr[i], col_ptr[i+1]) of `yc`.  All lanes of the warp must call it.
+#ifndef RB200_PRAQ_STAGE
+#define RB200_PRAQ_STAGE 256   // compile-time tunable (sweeps build with -D)
+#endif
+constexpr int kStage = RB200_PRAQ_STAGE;   // half-edge values a warp stages per pass
+
+// The sums of v over the runs [ptr[i], ptr[i+1]) of the 32 consecutive nodes
+// i = base + lane of a warp, one node per lane.  The runs of consecutive nodes
+// are adjacent, so the warp copies the whole range [ptr[base], ptr[base+32])
+// through shared memory in coalesced passes of kStage values, and each lane
+// adds its own run's part of every pass in order.  All lanes of the warp must
+// call it (with the same base).
+template <class Real, class Acc>
+__device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v, int n,
+                                         long long base, int lane, Real* __restrict__ stage) {
+    if (base >= n) return Acc(0);   // uniform over the warp
+    const long long i = base + lane;
+    const long long last = base + 32 < n ? base + 32 : n;
+    const int lo_all = ptr[base], hi_all = ptr[last];
+    int a = 0, b = 0;
+    if (i < n) {
+        a = ptr[i];
+        b = ptr[i + 1];
+    }
+    Acc s = Acc(0);
+    for (int c0 = lo_all; c0 < hi_all; c0 += kStage) {
+        const int c1 = min(hi_all, c0 + kStage);
+#pragma unroll 4
+        for (int k = c0 + lane; k < c1; k += 32) stage[k - c0] = v[k];
+        __syncwarp();
+        const int lo = max(a, c0), hi = min(b, c1);
+        for (int k = lo; k < hi; ++k) s += Acc(stage[k - c0]);
+        __syncwarp();
+    }
+    return s;
+}
+
+// S^T y at node base + lane: the node's run of `ys` (first-end order) plus its
+// run of `yc` (second-end order).
 template <class Real, class Acc>
 __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __restrict__ ys,
-                                          const Real* __restrict__ yc, long long i, int lane) {
-    Acc s0 = Acc(0), s1 = Acc(0);
-    if (i < d.n) {
-        const int L = d.lanes;
-        const int a = d.row_ptr[i], b = d.row_ptr[i + 1];
-        const int c = d.col_ptr[i], e = d.col_ptr[i + 1];
-        int k = a + lane, q = c + lane;
-        // both runs together, unrolled by two: four loads in flight
-        for (; k + L < b && q + L < e; k += 2 * L, q += 2 * L) {
-            const Real v0 = ys[k], v1 = ys[k + L], w0 = yc[q], w1 = yc[q + L];
-            s0 += Acc(v0) + Acc(v1);
-            s1 += Acc(w0) + Acc(w1);
-        }
-        for (; k < b; k += L) s0 += Acc(ys[k]);
-        for (; q < e; q += L) s1 += Acc(yc[q]);
-    }
-    Acc s = s0 + s1;
-    for (int o = d.lanes >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
+                                          const Real* __restrict__ yc, long long base, int lane,
+                                          Real* __restrict__ stage) {
+    const Acc s0 = warp_runs<Real, Acc>(d.row_ptr, ys, d.n, base, lane, stage);
+    const Acc s1 = warp_runs<Real, Acc>(d.col_ptr, yc, d.n, base, lane, stage);
+    return s0 + s1;
 }
 
 // Primal half of one PDHG step, with the Halpern combination of x folded in
@@ -144,10 +168,11 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
     __shared__ double scratch[kNodeSums * 32];
-    const long long g = (long long)tile * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & (d.lanes - 1);
-    const long long i = g >> d.lane_shift;
-    const bool owner = i < d.n && lane == 0;
+    __shared__ Real stage[kBlock / 32][kStage];
+    const int lane = threadIdx.x & 31;
+    const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
+    const long long i = base + lane;
+    const bool owner = i < d.n;
     // node data first, so its latency hides behind the gather
     Real x1o = Real(0), x2o = Real(0), x0o = Real(0), di = Real(0), dg = Real(1);
     if (owner) {
@@ -159,7 +184,7 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
             x0o = d.x0[i];
         }
     }
-    const Real s = scatter_at<Real, Real>(d, ys, yc, i, lane);
+    const Real s = scatter_at<Real, Real>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[kNodeSums] = {0.0, 0.0, 0.0};
     if (owner) {
         Real x1v;
@@ -286,12 +311,13 @@ template <class Real>
 __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     if (d.ctl->terminated) return;
     __shared__ double scratch[32];
-    const long long g = (long long)tile * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & (d.lanes - 1);
-    const long long i = g >> d.lane_shift;
-    const double s = scatter_at<Real, double>(d, ys, yc, i, lane);
+    __shared__ Real stage[kBlock / 32][kStage];
+    const int lane = threadIdx.x & 31;
+    const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
+    const long long i = base + lane;
+    const double s = scatter_at<Real, double>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[1] = {0.0};
-    if (i < d.n && lane == 0) {
+    if (i < d.n) {
         const double rc = double(d.diag[i]) - s;
         acc[0] = rc < 0.0 ? rc : 0.0;
     }
@@ -425,6 +451,55 @@ __global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta)
     }
 }
 
+// A warm start (qubo/praq-jax/praq/solver.py:482-560): the given primal
+// clipped to [0, 1]^n and the given half-edge dual pairs (instance units,
+// input edge order, wy[2e], wy[2e+1]) scaled and projected onto each edge's
+// dual set (projection.py:16-42), in the one-coordinate form.  NULL wx keeps
+// x = 1/2, NULL wy keeps the centroid.  Everything else as init_kernel.
+template <class Real>
+__global__ void warm_init_kernel(Dev<Real> d, Control* c, double omega, double theta,
+                                 const double* __restrict__ wx, const double* __restrict__ wy,
+                                 const int* __restrict__ perm) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < d.n) {
+        const Real x = wx ? Real(fmin(fmax(wx[k], 0.0), 1.0)) : Real(0.5);
+        d.x1[k] = x;
+        d.x2[k] = x;
+        d.x0[k] = x;
+    }
+    if (k < d.m) {
+        const Real sw = d.w[k];
+        Real u = Real(-0.5) * sw;
+        if (wy) {
+            const long long e = perm ? perm[k] : k;
+            const double sc = *d.scale;
+            const double v1 = wy[2 * e] / sc, v2 = wy[2 * e + 1] / sc, swd = double(sw);
+            u = swd > 0.0 ? Real(fmin(fmax(0.5 * (v1 + v2), -swd), 0.0))                  // covering
+                           : Real(fmin(fmax(v1 + 0.5 * (-swd - v1 - v2), 0.0), -swd));   // packing
+        }
+        const Real v = sw > Real(0) ? u : -sw - u;
+        d.u0[k] = u;
+        d.pred[k] = u;
+        d.u2s[k] = u;
+        d.predc[d.colpos[k]] = v;
+        d.u2c[d.colpos[k]] = v;
+    }
+    if (k == 0) {
+        c->omega = omega;
+        c->theta = theta;
+        c->fp_error = 0.0;
+        c->check_error = INFINITY;
+        c->new_error = 0.0;
+        c->lower = c->upper = c->gap = NAN;
+        c->restart_iter = 0;
+        c->iteration = 0;
+        c->terminated = 0;
+        c->restart = 0;
+        c->result_slot = 1;
+        c->status = 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // device preprocessing (the reference does this on the host:
 // qubo/praq-cuda/src/solver.cuh:517-569 and qubo/praq-cuda/src/praq.cu:35-79)
@@ -518,18 +593,10 @@ __global__ void prep_nodes_kernel(int n, const int* __restrict__ row_ptr, const 
     dn[i] = Real(diag[i] / *scale);
 }
 
-// Lanes per node: the smallest power of two (at most a warp) that leaves each
-// lane about four half-edges of the average degree.
-static int lanes_for(int n, int m) {
-    const double average = 2.0 * double(m) / double(n);
-    int lanes = 1;
-    while (lanes < 32 && double(lanes) * 4.0 < average) lanes *= 2;
-    return lanes;
-}
-
 struct SolverBase {
     virtual ~SolverBase() = default;
     virtual int run() = 0;
+    virtual int set_warm(const double* x, const double* y2) = 0;
     virtual int result(double* x, double* y2, PraqResult* r) = 0;
     virtual long long launches() const = 0;
     virtual int run_profiled(double* ms, long long* count) = 0;
@@ -547,6 +614,7 @@ struct Solver final : SolverBase {
     PoolBuf<int2> ends;
     PoolBuf<Real> w, diag, deg, x1, x2, x0, r, pred, predc, u0, u2s, u2c;
     PoolBuf<double> pnode, pedge, plower, scale;
+    PoolBuf<double> warm_x, warm_y;   // a warm start (instance units), optional
     PoolBuf<Control> ctl;
     Control* mirror = nullptr;   // pinned host copy of the control block
     Dev<Real> d{};
@@ -569,6 +637,7 @@ struct Solver final : SolverBase {
         x1.release(); x2.release(); x0.release(); r.release(); pred.release(); predc.release();
         u0.release(); u2s.release(); u2c.release();
         pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release();
+        warm_x.release(); warm_y.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -588,8 +657,7 @@ struct Solver final : SolverBase {
         if (!mirror) return PRAQ_ERROR_CUDA;
         const int st = layout(in);
         if (st) return st;
-        const int lanes = lanes_for(n, m);
-        nb_node = ceil_div((long long)n * lanes, kBlock);
+        nb_node = ceil_div(n, kBlock);   // one node per thread
         nb_edge = std::max(1, ceil_div(m, kBlock * kEdgesPerThread));
         for (auto* b : {&x1, &x2, &x0, &r})
             if (b->alloc(n, stream)) return PRAQ_ERROR_CUDA;
@@ -599,11 +667,15 @@ struct Solver final : SolverBase {
             pedge.alloc(size_t(nb_edge) * kEdgeSums, stream) || plower.alloc(nb_node, stream) ||
             ctl.alloc(1, stream))
             return PRAQ_ERROR_CUDA;
+        // With no edges no edge kernel ever writes its partial row, which the
+        // checks still read: it must hold zeros, not what the pool last held.
+        if (cudaMemsetAsync(pedge.ptr, 0, sizeof(double) * pedge.count, stream) ||
+            cudaMemsetAsync(pnode.ptr, 0, sizeof(double) * pnode.count, stream) ||
+            cudaMemsetAsync(plower.ptr, 0, sizeof(double) * plower.count, stream))
+            return PRAQ_ERROR_CUDA;
         for (auto& ev : done)
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return PRAQ_ERROR_CUDA;
-        d.n = n; d.m = m; d.lanes = lanes;
-        d.lane_shift = 0;
-        while ((1 << d.lane_shift) < lanes) ++d.lane_shift;
+        d.n = n; d.m = m;
         d.row_ptr = row_ptr.ptr; d.col_ptr = col_ptr.ptr; d.colpos = colpos.ptr;
         d.ends = ends.ptr; d.w = w.ptr; d.diag = diag.ptr; d.deg = deg.ptr; d.scale = scale.ptr;
         d.x1 = x1.ptr; d.x2 = x2.ptr; d.x0 = x0.ptr; d.r = r.ptr;
@@ -749,11 +821,26 @@ struct Solver final : SolverBase {
 
     cudaError_t launch_block() { return exec ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
 
-    // Cold start, the first vanilla step and the check before the loop.
+    // The start point of later runs: x [n] and dual pairs y2 [2m] (instance
+    // units, the input's edge order, as result() returns them); either may be
+    // null (x = 1/2, the centroid).  Both null: back to the cold start.
+    int set_warm(const double* x, const double* y2) override {
+        warm_x.release();
+        warm_y.release();
+        if (x && warm_x.upload(x, size_t(n), stream)) return PRAQ_ERROR_CUDA;
+        if (y2 && m && warm_y.upload(y2, size_t(2) * m, stream)) return PRAQ_ERROR_CUDA;
+        return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
+    }
+
+    // Cold (or warm) start, the first vanilla step and the check before the loop.
     int start_solve() {
         nlaunch = 0;
         const int count = std::max(n, m);
-        init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
+        if (warm_x.ptr || warm_y.ptr)
+            warm_init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(
+                d, d.ctl, p.omega, p.theta_initial, warm_x.ptr, warm_y.ptr, perm.ptr);
+        else
+            init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
         // x1, y1 = _raw_step(x0, y0): one vanilla step from the start, with
         // the sums for the error and the bounds at the start point.
         node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, 0, 1, 0);
@@ -886,32 +973,6 @@ struct Solver final : SolverBase {
     }
 
     long long launches() const override { return nlaunch; }
-
-    // Re-derive lanes per node for a target of `per_lane` half-edges per lane
-    // (the autotuner's knob); the partial-sum rows follow the node grid.
-    int set_lanes_target(double per_lane) {
-        const double average = 2.0 * double(m) / double(n);
-        int lanes = 1;
-        while (lanes < 32 && double(lanes) * per_lane < average) lanes *= 2;
-        if (lanes == d.lanes) return 0;
-        d.lanes = lanes;
-        d.lane_shift = 0;
-        while ((1 << d.lane_shift) < lanes) ++d.lane_shift;
-        nb_node = ceil_div((long long)n * lanes, kBlock);
-        if (pnode.alloc(size_t(nb_node) * kNodeSums, stream) || plower.alloc(nb_node, stream))
-            return PRAQ_ERROR_CUDA;
-        d.pnode = pnode.ptr;
-        d.plower = plower.ptr;
-        if (exec) {
-            cudaGraphExecDestroy(exec);
-            exec = nullptr;
-        }
-        if (graph) {
-            cudaGraphDestroy(graph);
-            graph = nullptr;
-        }
-        return 0;
-    }
 
     size_t device_bytes() const {
         size_t b = 0;

@@ -77,6 +77,11 @@ int reform_praq_result(reform_praq_solver* solver, double* x, double* y2, PraqRe
     return solver->impl->result(x, y2, result);
 }
 
+int reform_praq_set_warm(reform_praq_solver* solver, const double* x, const double* y2) {
+    if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
+    return solver->impl->set_warm(x, y2);
+}
+
 int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds) {
     if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
     solver->impl->time_limit = seconds;

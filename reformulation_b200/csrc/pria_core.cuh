@@ -61,6 +61,7 @@ constexpr int kXThreads = 256;
 constexpr int kAuxThreads = 256;
 constexpr int kCheckBlock = 256;
 constexpr int kLowTW = 32;              // columns per tile of the lower-bound pass
+constexpr int kXTile = 16;              // columns per tile of the x half-step (FP64 tile)
 constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
 constexpr int kMaxCluster = 16;
 constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
@@ -219,8 +220,12 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
          int step, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
+    // The tile of pre = x - tau (h + y + z) is FP64 whatever Real is: tau h
+    // can exceed x by many orders of magnitude (the duals' scale is K / scale
+    // per entry, the primal's is 1), and the column threshold cancels that
+    // common part, so pre must carry the digits FP32 would drop.
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* pre = reinterpret_cast<Real*>(smem_raw);
+    double* pre = reinterpret_cast<double*>(smem_raw);
     __shared__ double theta[TW];
     __shared__ double scratch[2 * 32];
     const int item = tile % d.n;
@@ -234,7 +239,7 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
     const int col = lane % TW, sub = lane / TW;
     const int tt = t0 + col;
     const double om = c->omega;
-    const Real tau = Real(d.eta / om), sigma = Real(d.eta * om);
+    const double tau = d.eta / om, sigma = d.eta * om;
     // rows are taken kUnroll at a time per warp so that their loads are in
     // flight together
     const int rstep = nwarps * kRpw;
@@ -255,7 +260,9 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u)
-            if (ev[u] >= 0) pre[col * stride + sb + u * rstep] = xv[u] - tau * ((hv[u] + yv[u]) + zv[u]);
+            if (ev[u] >= 0)
+                pre[col * stride + sb + u * rstep] =
+                    double(xv[u]) - tau * ((double(hv[u]) + double(yv[u])) + double(zv[u]));
     }
     __syncthreads();
     for (int cc = warp; cc < tcols; cc += nwarps) {
@@ -268,7 +275,7 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
     }
     __syncthreads();
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
-    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    const double lwn = kn / (kn + 1.0), rwn = 1.0 / (kn + 1.0);
     // Without Reflect: a vanilla step (the next point is the step itself and
     // the anchor stays), or the step that makes the point stepped from the
     // new anchor (restart; the end of the vanilla phase, whose drift sums are
@@ -293,10 +300,11 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
         for (int u = 0; u < kUnroll; ++u) {
             if (ev[u] < 0) continue;
             const long long e = ev[u];
-            const Real x2 = Real(fmax(double(pre[col * stride + sb + u * rstep]) - theta[col], 0.0));
+            const Real x2 = Real(fmax(pre[col * stride + sb + u * rstep] - theta[col], 0.0));
             const Real x1 = x1v[u], xa = Reflect ? xav[u] : x1;
-            d.r[e] = sigma * (Real(2) * x2 - x1);
-            d.xh[e] = vanilla ? x2 : lwn * (Real(2) * x2 - x1) + rwn * xa;
+            const double refl = 2.0 * double(x2) - double(x1);
+            d.r[e] = Real(sigma * refl);
+            d.xh[e] = vanilla ? x2 : Real(lwn * refl + rwn * double(xa));
             if (!Reflect && !vanilla) d.x0[e] = x1;
             if (Check) {
                 d.x2s[e] = x2;
@@ -745,7 +753,7 @@ __global__ void warm_pack_kernel(Dev<Real> d, const double* __restrict__ wx, con
 template <class Real, int TW>
 __global__ void __launch_bounds__(kXThreads) project_x_kernel(Dev<Real> d, Real* x) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* pre = reinterpret_cast<Real*>(smem_raw);
+    double* pre = reinterpret_cast<double*>(smem_raw);
     __shared__ double theta[TW];
     const int item = blockIdx.x % d.n;
     const int ctile = d.ntc - 1 - int(blockIdx.x / d.n);
@@ -768,7 +776,7 @@ __global__ void __launch_bounds__(kXThreads) project_x_kernel(Dev<Real> d, Real*
     for (int s = warp * kRpw + sub; s < rows; s += nwarps * kRpw)
         if (col < tcols && tt >= s)
             x[blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s)] =
-                Real(fmax(double(pre[col * stride + s]) - theta[col], 0.0));
+                Real(fmax(pre[col * stride + s] - theta[col], 0.0));
 }
 
 template <class Real>
@@ -938,7 +946,7 @@ struct Solver final : SolverBase {
     PoolBuf<Control> ctl;
     Control* mirror = nullptr;
     Dev<Real> d{};
-    int tw = 32, nbx = 1, nbyz = 1, nblo = 1;
+    int tw = kXTile, nbx = 1, nbyz = 1, nblo = 1;
     size_t x_smem = 0, yz_smem = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -946,9 +954,10 @@ struct Solver final : SolverBase {
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
     static constexpr int kYZThreads = 256;
-    // x tiles: tw columns of a padded row of at most kMaxPeriods (+1) reals
+    // x tiles: kXTile columns of a padded row of at most kMaxPeriods (+1)
+    // FP64 values
     static constexpr size_t x_smem_limit() {
-        return size_t(sizeof(Real) == 4 ? 32 : 16) * size_t(kMaxPeriods + 1) * sizeof(Real);
+        return size_t(kXTile) * size_t(kMaxPeriods + 1) * sizeof(double);
     }
 
     ~Solver() override {
@@ -1053,12 +1062,12 @@ struct Solver final : SolverBase {
     cudaError_t setup_common() {
         for (auto* b : {&xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s})
             RB_CUDA_TRY(b->alloc(nd, stream));
-        tw = sizeof(Real) == 4 ? 32 : 16;
+        tw = kXTile;
         const int ntc = (tp + tw - 1) / tw;
         const int ntc_low = (tp + kLowTW - 1) / kLowTW;
         nbx = n * ntc;
         nblo = n * ntc_low;
-        x_smem = size_t(tw) * size_t(tp | 1) * sizeof(Real);
+        x_smem = size_t(tw) * size_t(tp | 1) * sizeof(double);
         int csize = 1;
         while (csize < kMaxCluster && (size_t((n + csize - 1) / csize) * tp * sizeof(Real)) > size_t(kSliceBytes))
             ++csize;
@@ -1122,24 +1131,16 @@ struct Solver final : SolverBase {
     }
     cudaError_t set_attributes() {
         if (x_smem > x_smem_limit()) return cudaErrorInvalidValue;
-        if (tw == 32) {
-            RB_CUDA_TRY((x_attr<32, true, false>()));
-            RB_CUDA_TRY((x_attr<32, true, true>()));
-            RB_CUDA_TRY((x_attr<32, false, true>()));
-            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(x_smem_limit())));
-        } else {
-            RB_CUDA_TRY((x_attr<16, true, false>()));
-            RB_CUDA_TRY((x_attr<16, true, true>()));
-            RB_CUDA_TRY((x_attr<16, false, true>()));
-            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(x_smem_limit())));
-        }
+        RB_CUDA_TRY((x_attr<kXTile, true, false>()));
+        RB_CUDA_TRY((x_attr<kXTile, true, true>()));
+        RB_CUDA_TRY((x_attr<kXTile, false, true>()));
+        RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, kXTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(x_smem_limit())));
         RB_CUDA_TRY((yz_attr<true, false>()));
         RB_CUDA_TRY((yz_attr<true, true>()));
         RB_CUDA_TRY((yz_attr<false, true>()));
         if (vanilla_phase()) {
-            RB_CUDA_TRY(tw == 32 ? (x_attr<32, false, false>()) : (x_attr<16, false, false>()));
+            RB_CUDA_TRY((x_attr<kXTile, false, false>()));
             RB_CUDA_TRY((yz_attr<false, false>()));
         }
         return cudaSuccess;
@@ -1151,10 +1152,7 @@ struct Solver final : SolverBase {
 
     template <bool R, bool C>
     cudaError_t launch_x(const Real* xs, const Real* ys, const Real* zs, int step, int gate) {
-        if (tw == 32)
-            x_kernel<Real, 32, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
-        else
-            x_kernel<Real, 16, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
+        x_kernel<Real, kXTile, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
         return cudaGetLastError();
     }
 
@@ -1264,10 +1262,7 @@ struct Solver final : SolverBase {
         if (has_warm) {
             warm_pack_kernel<Real><<<tp, 256, 0, stream>>>(d, warm[0].ptr, warm[1].ptr, warm[2].ptr, d.x0, d.y0,
                                                            d.z0);
-            if (tw == 32)
-                project_x_kernel<Real, 32><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, d.x0);
-            else
-                project_x_kernel<Real, 16><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, d.x0);
+            project_x_kernel<Real, kXTile><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, d.x0);
             project_yz_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.y0, d.z0);
             nlaunch += 3;
         }
@@ -1339,8 +1334,8 @@ struct Solver final : SolverBase {
                 if ((st = cudaEventSynchronize(done[kk])) != cudaSuccess) return int(st);
                 if (mirror->terminated) break;
                 if (p.verbose)
-                    fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e\n",
-                            mirror->iteration, mirror->upper, mirror->lower, mirror->gap);
+                    fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  omega %.3e\n",
+                            mirror->iteration, mirror->upper, mirror->lower, mirror->gap, mirror->omega);
                 if ((st = launch_block()) != cudaSuccess) return int(st);
                 if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
                 nlaunch += block_nodes;

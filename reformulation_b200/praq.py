@@ -7,6 +7,8 @@
   again from the cold start (the timing harness and the serving engine use it).
 * `solve(instance, *, tolerances, time_limit, ...)` is the backend entry point,
   the drop-in for ``qubo/harness/backends/praq_cuda.py:79-167``.
+* `solve_warm_start`, `relaxation_bounds` and `persistent_variables` are the
+  reference's post-solve API (``qubo/praq-jax/praq/solver.py:348-362,482-611``).
 """
 
 from __future__ import annotations
@@ -111,6 +113,20 @@ class DeviceSolver:
     def set_time_limit(self, seconds: float) -> None:
         self._lib.reform_praq_set_time_limit(self._h, float(seconds))
 
+    def set_warm(self, x=None, y=None) -> None:
+        """Start later runs from (x, y) instead of the centroid: x [n] and the
+        dual pairs y [m, 2] (or [2m]) in instance units, edge order of the
+        instance; both are projected.  None keeps that part cold."""
+        self._warm = [None if a is None else np.ascontiguousarray(a, np.float64).ravel() for a in (x, y)]
+        if self._warm[0] is not None and self._warm[0].size != self.n:
+            raise ValueError("warm x must have n entries")
+        if self._warm[1] is not None and self._warm[1].size != 2 * self.m:
+            raise ValueError("warm y must have 2m entries")
+        rc = self._lib.reform_praq_set_warm(self._h, *[_native.dptr(a) if a is not None else None
+                                                       for a in self._warm])
+        if rc != 0:
+            raise RuntimeError(f"reform_praq_set_warm failed with status {rc}")
+
     def run(self) -> int:
         return int(self._lib.reform_praq_run(self._h))
 
@@ -156,6 +172,47 @@ class DeviceSolver:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def solve_warm_start(instance, parameters: _native.PraqParameters, warm_start) -> tuple:
+    """Solve from a given point, as the reference's solve_qubo_problem_warm_start
+    (qubo/praq-jax/praq/solver.py:482-560): `warm_start` = (x, y), x [n] and
+    dual pairs y [m, 2] in instance units, both projected before use.  Returns
+    (primal [n], dual [m, 2] in instance units, iterations)."""
+    with DeviceSolver(instance, parameters) as dev:
+        dev.set_warm(*warm_start)
+        code = dev.run()
+        if code < 0:
+            raise RuntimeError(f"reform_praq_run failed with status {code}")
+        res, y = dev.result(want_x=True, want_dual=True)
+    return res.x, y, res.iterations
+
+
+def relaxation_bounds(instance, primal, dual) -> tuple[float, float]:
+    """(lower, upper) bracket of the relaxation value from a feasible
+    primal-dual pair, in instance units (qubo/praq-jax/praq/solver.py:348-362):
+    lower = L_D(dual), upper = F(primal).  Evaluated on the device by the
+    solver's own bound kernels at the pair (the check before the first step of
+    a solve started there); the pair is projected first, which leaves a
+    feasible pair as it is."""
+    p = _native.lib().praq_default_parameters()
+    p.tolerance = math.inf      # the check at the start point ends the run
+    with DeviceSolver(instance, p) as dev:
+        dev.set_warm(primal, dual)
+        code = dev.run()
+        if code < 0:
+            raise RuntimeError(f"reform_praq_run failed with status {code}")
+        res = dev.result(want_x=False)
+    return res.lower, res.upper
+
+
+def persistent_variables(primal, tolerance: float = 1e-6) -> tuple[np.ndarray, np.ndarray]:
+    """The coordinates a relaxation optimum fixes by persistency of the roof
+    dual, and their values (qubo/praq-jax/praq/solver.py:592-611): (mask of
+    coordinates within `tolerance` of 0 or 1, rounded values)."""
+    x = np.asarray(primal, dtype=np.float64)
+    rounded = np.round(x)
+    return np.abs(x - rounded) <= tolerance, rounded
 
 
 def solve(instance, *, tolerances: Tolerances = Tolerances(), time_limit: float = math.inf,

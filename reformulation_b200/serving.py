@@ -1,7 +1,8 @@
 """A continuous-batching request loop over the batched engine.
 
 Requests (QUBO roof-dual LPs and JRP LPs) arrive over time.  The server keeps
-one engine (`batch.Batch`, FP32 iterates with FP64 reductions by default):
+one engine (`batch.EscalatingBatch`, FP32 iterates with FP64 reductions by
+default, a QUBO that stalls in FP32 continuing in FP64 from its last point):
 
 * a request is ADMITTED as soon as the device-memory budget allows (its
   footprint is estimated from its size before it is laid out), between two
@@ -29,7 +30,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import praq, pria
-from .batch import Batch
+from .batch import Batch, EscalatingBatch
 from .instances import JrpSpec, QuboInstance
 
 
@@ -84,14 +85,15 @@ class Server:
     tolerance: float = 1e-4
     max_iter: int = 200_000
     blocks_in_flight: int = 2
-    batch: Batch = field(init=False)
+    batch: Batch | EscalatingBatch = field(init=False)
     waiting: deque = field(default_factory=deque)
     running: dict = field(default_factory=dict)   # engine id -> (Request, admitted time)
     done: list = field(default_factory=list)
     high_water: int = 0
 
     def __post_init__(self):
-        self.batch = Batch(self.precision)
+        # mixed: FP32 iterates, with QUBOs that stall in FP32 continued in FP64
+        self.batch = EscalatingBatch() if self.precision == "mixed" else Batch(self.precision)
         self._qp = praq.Library().parameters(tolerance=self.tolerance, max_iter=self.max_iter,
                                              use_float32=int(self.precision == "mixed"))
         self._jp = pria.Library().parameters(self.max_iter, self.tolerance)

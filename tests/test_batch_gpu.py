@@ -145,3 +145,53 @@ def test_long_horizon_added_before_short_ones(native):
         for i, j in zip(ids, sj):
             r = b.result_jrp(i)
             assert r.iterations == j.iterations and r.primal_objective == j.primal_objective
+
+
+def test_warm_start_and_point_in_batch(native):
+    """A warm-started QUBO in the batch equals the same warm start solo
+    (bitwise); the point of a running instance can be read and the instance
+    removed while others continue."""
+    from reformulation_b200 import praq
+    from reformulation_b200.batch import Batch
+    qs, js = mix()
+    lib = praq.Library()
+    p = lib.parameters(tolerance=1e-6, max_iter=20000)
+    rng = np.random.default_rng(9)
+    warm = (rng.uniform(0, 1, qs[1].n), rng.normal(0, 20, (qs[1].edges, 2)))
+    with praq.DeviceSolver(qs[1], p) as dev:
+        dev.set_warm(*warm)
+        assert dev.run() == 0
+        solo = dev.result()
+    with Batch("fp64") as b:
+        a = b.add_qubo(qs[1], p)
+        c = b.add_qubo(qs[3], p)
+        b.set_warm_qubo(a, *warm)
+        b.start()
+        b.launch()
+        b.sync()
+        x, y = b.point_qubo(c)
+        assert x.shape == (qs[3].n,) and y.shape == (qs[3].edges, 2)
+        assert np.all((x >= 0) & (x <= 1))
+        b.remove(c)                      # running: leaves the schedule
+        b.run()
+        r = b.result_qubo(a)
+        assert r.iterations == solo.iterations and r.upper == solo.upper and r.lower == solo.lower
+
+
+def test_escalation_continues_stalled_qubos_in_fp64(native, oracle_lib):
+    """FP32 iterates cannot reach a 1e-8 gap; the escalating batch moves such a
+    QUBO to FP64 at its last point and finishes it there, to the oracle's
+    optimum.  A JRP in the same batch stays in FP32."""
+    from reformulation_b200.batch import EscalatingBatch
+    qs, js = mix()
+    with EscalatingBatch(stall_iterations=256) as b:
+        i = b.add_qubo(qs[2], qp(1e-8))
+        k = b.add_jrp(js[0], jp(1e-4))
+        b.start()
+        b.run()
+        assert i in b.escalated and k not in b.escalated
+        r = b.result_qubo(i)
+        assert r.status == 0 and (r.upper - r.lower) / (1 + abs(r.upper) + abs(r.lower)) <= 1e-8
+        flow = oracle_lib.roof_dual_maxflow(qs[2])
+        assert rel(r.upper, flow) <= 1e-7
+        assert b.status(k)[0] and b.result_jrp(k).relative_gap <= 1e-4

@@ -202,3 +202,41 @@ def test_unsorted_and_reversed_edges(lib, oracle_lib):
         res, y = dev.result(want_dual=True)
     low = oracle_lib.qubo_lower_bound(shuffled, y)
     assert rel(low, res.lower) <= 1e-9
+
+
+def test_warm_start_and_relaxation_bounds(native, oracle_lib):
+    """The warm-start API of qubo/praq-jax/praq/solver.py:482-560: from the
+    optimum it ends at the check before the first step; from any point
+    (projected) it reaches the same optimum.  relaxation_bounds at the
+    returned pair is the bracket the solver reported (solver.py:348-362)."""
+    from reformulation_b200 import praq
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    lib = praq.Library()
+    p = lib.parameters(tolerance=1e-9)
+    with praq.DeviceSolver(inst, p) as dev:
+        assert dev.run() == 0
+        cold, y = dev.result(want_x=True, want_dual=True)
+    lo, up = praq.relaxation_bounds(inst, cold.x, y)
+    assert rel(lo, cold.lower) <= 1e-12 and rel(up, cold.upper) <= 1e-12
+    x, y2, its = praq.solve_warm_start(inst, p, (cold.x, y))
+    assert its == 0 and np.array_equal(x, cold.x)
+    rng = np.random.default_rng(3)
+    far = (rng.uniform(-1, 2, inst.n), rng.normal(0, 50, (inst.edges, 2)))
+    x, y2, its = praq.solve_warm_start(inst, p, far)
+    lo, up = praq.relaxation_bounds(inst, x, y2)
+    flow = oracle_lib.roof_dual_maxflow(inst)
+    assert its > 0 and lo <= flow + 1e-7 * (1 + abs(flow)) <= up + 2e-7 * (1 + abs(flow))
+    assert rel(up, flow) <= 1e-7
+    assert np.all((x >= 0) & (x <= 1))
+    fixed, vals = praq.persistent_variables(x)
+    assert fixed.any() and set(np.unique(vals[fixed])) <= {0.0, 1.0}
+
+
+def test_edgeless_instance_terminates(lib):
+    """No edges: the edge partial sums the checks read are zeros (not stale
+    pool memory), so the solve ends."""
+    inst = QuboInstance("e", "e", 5, np.array([-2.0, 1.0, 3.0, -1.0, 0.0]), np.zeros(0, np.int64),
+                        np.zeros(0, np.int64), np.zeros(0))
+    for _ in range(3):
+        s = lib.solve(inst, lib.parameters(tolerance=1e-9, max_iter=10_000))
+        assert s.status == 0 and abs(s.upper - (-3.0)) <= 1e-8
