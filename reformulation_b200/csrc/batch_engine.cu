@@ -39,7 +39,7 @@ struct QMeta {
 };
 struct JMeta {
     pria::Params prm;
-    int nbx, nbyz, nbup, nblo;
+    int nbx, nby, nbyz, nbup, nblo;
 };
 
 // One instance's state as the host needs it after a block.
@@ -49,7 +49,14 @@ struct Summary {
     int terminated, restart;
 };
 
-enum Count { kNode = 0, kEdge, kQLow, kX, kUp, kJLow, kQCheck, kJCheck, kYZ0 };
+// JRP x tiles fall into classes by the shared memory they need (their row
+// count), each class launched with its own dynamic shared memory, so that the
+// longest horizon in the batch does not set every tile's occupancy.
+constexpr int kXClasses = 4;
+constexpr int kXClassRows[kXClasses] = {127, 255, 511, pria::kMaxPeriods + 1};   // rows | 1 at most
+
+enum Count { kNode = 0, kEdge, kQLow, kUp, kJLow, kQCheck, kJCheck, kY, kX0 };
+constexpr int kYZ0 = kX0 + kXClasses;
 constexpr int kMaxGroups = 17;   // y/z cluster sizes 1..16
 constexpr int kCounts = kYZ0 + kMaxGroups;
 
@@ -129,12 +136,28 @@ bj_x(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* cou
     }
 }
 
+template <class Real, bool Reflect, bool Check>
+__global__ void __launch_bounds__(pria::kYThreads)
+bj_y(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
+    __shared__ pria::Dev<Real> sd;
+    extern __shared__ __align__(16) unsigned char smem_raw[];   // kYThreads / 32 rows of kMaxPeriods
+    const int total = *count;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int2 w = tiles[t];
+        __syncthreads();
+        if (threadIdx.x == 0) sd = devs[w.x];
+        __syncthreads();
+        pria::y_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? sd.yh : sd.y2s, step, gate,
+                                                  reinterpret_cast<Real*>(smem_raw), pria::kMaxPeriods);
+    }
+}
+
 // Persistent clusters: cluster c takes tasks c, c + clusters, ...; every CTA
-// of a cluster takes the same task (the y/z half-step of one period block).
+// of a cluster takes the same task (the z half-step of one period block).
 template <class Real, int kThreads, bool Reflect, bool Check>
 __global__ void __launch_bounds__(kThreads)
-bj_yz(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count, int csize, int step,
-      int gate) {
+bj_z(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count, int csize, int step,
+     int gate) {
     __shared__ pria::Dev<Real> sd;
     const int total = *count;
     const int nclusters = int(gridDim.x) / csize;
@@ -143,10 +166,7 @@ bj_yz(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* co
         __syncthreads();
         if (threadIdx.x == 0) sd = devs[w.x];
         __syncthreads();
-        if (Reflect)
-            pria::yz_task<Real, kThreads, Reflect, Check>(sd, w.y, sd.yh, sd.zh, step, gate);
-        else
-            pria::yz_task<Real, kThreads, Reflect, Check>(sd, w.y, sd.y2s, sd.z2s, step, gate);
+        pria::z_task<Real, kThreads, Reflect, Check>(sd, w.y, Reflect ? sd.zh : sd.z2s, step, gate);
     }
 }
 
@@ -187,7 +207,7 @@ bj_check(const pria::Dev<Real>* devs, const JMeta* metas, const int* __restrict_
         const int id = list[k];
         const pria::Dev<Real>& d = devs[id];
         const JMeta& m = metas[id];
-        pria::check_body(d.ctl, m.prm, d.px, m.nbx, d.pyz, m.nbyz, d.pup, m.nbup, d.plo, m.nblo, mode);
+        pria::check_body(d.ctl, m.prm, d.px, m.nbx, d.py, m.nby, d.pyz, m.nbyz, d.pup, m.nbup, d.plo, m.nblo, mode);
         __syncthreads();
     }
 }
@@ -279,7 +299,8 @@ struct Engine final : EngineBase {
     Table<QMeta> qmeta;
     Table<pria::Dev<Real>> jdevs;
     Table<JMeta> jmeta;
-    Table<int2> t_node, t_edge, t_qlow, t_x, t_up, t_jlow;
+    Table<int2> t_node, t_edge, t_qlow, t_up, t_jlow, t_y;
+    Table<int2> t_x[kXClasses];
     Table<int2> t_yz[kMaxGroups];
     Table<int> l_qcheck, l_jcheck;
     Table<unsigned char> live;
@@ -289,8 +310,10 @@ struct Engine final : EngineBase {
     size_t hsummary_cap = 0;
     int hcounts[kCounts] = {};
 
-    size_t x_smem = 0, yz_smem[kMaxGroups] = {};
+    size_t yz_smem[kMaxGroups] = {};
     bool groups[kMaxGroups] = {};
+    bool xclasses[kXClasses] = {};
+    bool graph_q = false, graph_j = false;   // the captured block has QUBO / JRP work
     static constexpr int tw = pria::kXTile;
     bool dirty = true;          // the graph must be captured again
     cudaGraph_t graph = nullptr;
@@ -304,6 +327,11 @@ struct Engine final : EngineBase {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         for (auto ev : events) cudaEventDestroy(ev);
+        for (auto ev : fj) cudaEventDestroy(ev);
+        for (auto st : aux) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         q.clear();
         j.clear();
         // every stream-ordered free before the stream goes away
@@ -311,7 +339,8 @@ struct Engine final : EngineBase {
         qmeta.buf.release();
         jdevs.buf.release();
         jmeta.buf.release();
-        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow}) tb->buf.release();
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_up, &t_jlow, &t_y}) tb->buf.release();
+        for (auto& tb : t_x) tb.buf.release();
         for (auto& tb : t_yz) tb.buf.release();
         l_qcheck.buf.release();
         l_jcheck.buf.release();
@@ -419,15 +448,16 @@ struct Engine final : EngineBase {
         for (auto& ji : j) {
             jdevs.host.push_back(ji.s ? ji.s->d : pria::Dev<Real>{});
             JMeta m{};
-            if (ji.s) m = JMeta{ji.s->prm, ji.s->nbx, ji.s->nbyz, ji.s->tp, ji.s->nblo};
+            if (ji.s) m = JMeta{ji.s->prm, ji.s->nbx, ji.s->nby, ji.s->nbyz, ji.s->tp, ji.s->nblo};
             jmeta.host.push_back(m);
         }
-        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow}) tb->host.clear();
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_up, &t_jlow, &t_y}) tb->host.clear();
+        for (auto& tb : t_x) tb.host.clear();
         for (auto& tb : t_yz) tb.host.clear();
         l_qcheck.host.clear();
         l_jcheck.host.clear();
         live.host.assign(q.size() + j.size(), 0);
-        size_t xs = 0, ys[kMaxGroups] = {};
+        size_t ys[kMaxGroups] = {};
         bool gr[kMaxGroups] = {};
         for (int k = 0; k < int(q.size()); ++k) {
             auto& qi = q[k];
@@ -442,7 +472,7 @@ struct Engine final : EngineBase {
             l_qcheck.host.push_back(k);
         }
         // JRP: x tiles sorted by rows (cost), y/z tasks by block size
-        std::vector<std::pair<long long, int2>> xt, yzt[kMaxGroups], upt;
+        std::vector<std::pair<long long, int2>> xt[kXClasses], yzt[kMaxGroups], upt, yt;
         for (int k = 0; k < int(j.size()); ++k) {
             auto& ji = j[k];
             if (!ji.s || !ji.started || ji.done) continue;
@@ -451,7 +481,10 @@ struct Engine final : EngineBase {
             const int n = s.n, tp = s.tp, ntc = s.d.ntc;
             for (int t = 0; t < n * ntc; ++t) {
                 const int ctile = ntc - 1 - t / n;
-                xt.emplace_back((long long)std::min(tp, (ctile + 1) * s.tw), make_int2(k, t));
+                const int rows = std::min(tp, (ctile + 1) * s.tw);
+                int cls = 0;
+                while ((rows | 1) > kXClassRows[cls]) ++cls;
+                xt[cls].emplace_back((long long)rows, make_int2(k, t));
             }
             const int c = s.d.csize;
             gr[c] = true;
@@ -461,15 +494,31 @@ struct Engine final : EngineBase {
                 upt.emplace_back((long long)n * (tp - sb), make_int2(k, sb));
             }
             for (int t = 0; t < s.nblo; ++t) t_jlow.host.push_back(make_int2(k, t));
-            xs = std::max(xs, s.x_smem);
+            for (int t = 0; t < s.nby; ++t) {
+                const long long row = (long long)t * (pria::kYThreads / 32);
+                yt.emplace_back((long long)(tp - int(row / n)), make_int2(k, t));   // row length
+            }
             l_jcheck.host.push_back(k);
         }
         auto order = [](std::vector<std::pair<long long, int2>>& v, Table<int2>& out) {
             std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
             for (auto& e : v) out.host.push_back(e.second);
         };
-        order(xt, t_x);
+        const bool run_q = !l_qcheck.host.empty(), run_j = !l_jcheck.host.empty();
+        if (run_q != graph_q || run_j != graph_j) {
+            graph_q = run_q;
+            graph_j = run_j;
+            dirty = true;
+        }
+        for (int c = 0; c < kXClasses; ++c) {
+            order(xt[c], t_x[c]);
+            if (!xt[c].empty() && !xclasses[c]) {
+                xclasses[c] = true;
+                dirty = true;
+            }
+        }
         order(upt, t_up);
+        order(yt, t_y);
         for (int c = 1; c < kMaxGroups; ++c) order(yzt[c], t_yz[c]);
         for (int c = 1; c < kMaxGroups; ++c) {
             if (gr[c] && (!groups[c] || ys[c] > yz_smem[c])) dirty = true;
@@ -478,23 +527,22 @@ struct Engine final : EngineBase {
                 yz_smem[c] = std::max(yz_smem[c], ys[c]);
             }
         }
-        if (xs > x_smem) {
-            x_smem = xs;
-            dirty = true;
-        }
         int rc = 0;
         if ((rc = upload(qdevs)) || (rc = upload(qmeta)) || (rc = upload(jdevs)) || (rc = upload(jmeta))) return rc;
-        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_x, &t_up, &t_jlow})
+        for (auto* tb : {&t_node, &t_edge, &t_qlow, &t_up, &t_jlow, &t_y})
             if ((rc = upload(*tb))) return rc;
+        for (int c = 0; c < kXClasses; ++c)
+            if (xclasses[c] && (rc = upload(t_x[c]))) return rc;
         for (int c = 1; c < kMaxGroups; ++c)
             if (groups[c] && (rc = upload(t_yz[c]))) return rc;
         if ((rc = upload(l_qcheck)) || (rc = upload(l_jcheck)) || (rc = upload(live))) return rc;
         hcounts[kNode] = int(t_node.host.size());
         hcounts[kEdge] = int(t_edge.host.size());
         hcounts[kQLow] = int(t_qlow.host.size());
-        hcounts[kX] = int(t_x.host.size());
+        for (int c = 0; c < kXClasses; ++c) hcounts[kX0 + c] = int(t_x[c].host.size());
         hcounts[kUp] = int(t_up.host.size());
         hcounts[kJLow] = int(t_jlow.host.size());
+        hcounts[kY] = int(t_y.host.size());
         hcounts[kQCheck] = int(l_qcheck.host.size());
         hcounts[kJCheck] = int(l_jcheck.host.size());
         for (int c = 0; c < kMaxGroups; ++c) hcounts[kYZ0 + c] = int(t_yz[c].host.size());
@@ -518,24 +566,35 @@ struct Engine final : EngineBase {
         return 0;
     }
 
+    static constexpr size_t x_class_smem(int c) { return size_t(tw) * size_t(kXClassRows[c]) * sizeof(double); }
+
     template <bool R, bool C>
-    cudaError_t launch_x(int step, int gate) {
-        const int grid = std::max(1, sms * std::max(1, int((228 * 1024) / std::max<size_t>(x_smem + 2048, 1))));
-        bj_x<Real, tw, R, C><<<grid, pria::kXThreads, x_smem, stream>>>(jdevs.buf.ptr, t_x.buf.ptr,
-                                                                     counts.ptr + kX, step, gate);
+    cudaError_t launch_x(int c, int step, int gate, cudaStream_t st) {
+        const size_t smem = x_class_smem(c);
+        const int per_sm = std::max(1, std::min(8, int((228 * 1024) / (smem + 2048))));
+        bj_x<Real, tw, R, C><<<sms * per_sm, pria::kXThreads, smem, st>>>(jdevs.buf.ptr, t_x[c].buf.ptr,
+                                                                         counts.ptr + kX0 + c, step, gate);
         return cudaGetLastError();
     }
 
     template <bool R, bool C>
-    cudaError_t launch_yz(int c, int step, int gate) {
-        constexpr int kT = pria::Solver<Real>::kYZThreads;
+    cudaError_t launch_y(int step, int gate, cudaStream_t st) {
+        const size_t smem = pria::Solver<Real>::y_smem_limit();
+        bj_y<Real, R, C><<<sms * std::max(1, int((228 * 1024) / (smem + 2048))), pria::kYThreads, smem, st>>>(
+            jdevs.buf.ptr, t_y.buf.ptr, counts.ptr + kY, step, gate);
+        return cudaGetLastError();
+    }
+
+    template <bool R, bool C>
+    cudaError_t launch_yz(int c, int step, int gate, cudaStream_t st) {
+        constexpr int kT = pria::kZThreads;
         const int per_sm = std::max(1, int((228 * 1024) / (yz_smem[c] + 4096)));
         const int nclusters = std::max(1, (sms * std::min(per_sm, 2)) / c);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(unsigned(nclusters * c));
         cfg.blockDim = dim3(kT);
         cfg.dynamicSmemBytes = yz_smem[c];
-        cfg.stream = stream;
+        cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = unsigned(c);
@@ -543,7 +602,7 @@ struct Engine final : EngineBase {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, bj_yz<Real, kT, R, C>, (const pria::Dev<Real>*)jdevs.buf.ptr,
+        return cudaLaunchKernelEx(&cfg, bj_z<Real, kT, R, C>, (const pria::Dev<Real>*)jdevs.buf.ptr,
                                   (const int2*)t_yz[c].buf.ptr, (const int*)(counts.ptr + kYZ0 + c), c, step,
                                   gate);
     }
@@ -553,76 +612,156 @@ struct Engine final : EngineBase {
     // in the process (the same rule as the single-instance solver's).
     cudaError_t set_attributes() {
         const size_t xlim = pria::Solver<Real>::x_smem_limit();
-        if (x_smem > xlim) return cudaErrorInvalidValue;
+        static_assert(x_class_smem(kXClasses - 1) <= pria::Solver<Real>::x_smem_limit(), "x class fits");
         auto xa = [&](auto fn) {
             return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(xlim));
         };
         RB_CUDA_TRY(xa(bj_x<Real, tw, true, false>));
         RB_CUDA_TRY(xa(bj_x<Real, tw, true, true>));
         RB_CUDA_TRY(xa(bj_x<Real, tw, false, true>));
-        constexpr int kT = pria::Solver<Real>::kYZThreads;
+        auto yattr = [&](auto fn) {
+            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(pria::Solver<Real>::y_smem_limit()));
+        };
+        RB_CUDA_TRY(yattr(bj_y<Real, true, false>));
+        RB_CUDA_TRY(yattr(bj_y<Real, true, true>));
+        RB_CUDA_TRY(yattr(bj_y<Real, false, true>));
+        constexpr int kT = pria::kZThreads;
         auto ya = [&](auto fn) -> cudaError_t {
             RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pria::kSliceBytes));
             return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         };
-        RB_CUDA_TRY(ya(bj_yz<Real, kT, true, false>));
-        RB_CUDA_TRY(ya(bj_yz<Real, kT, true, true>));
-        RB_CUDA_TRY(ya(bj_yz<Real, kT, false, true>));
+        RB_CUDA_TRY(ya(bj_z<Real, kT, true, false>));
+        RB_CUDA_TRY(ya(bj_z<Real, kT, true, true>));
+        RB_CUDA_TRY(ya(bj_z<Real, kT, false, true>));
         return cudaSuccess;
     }
 
+    // --- fork/join on auxiliary streams (graph branches under capture) -----
+    std::vector<cudaStream_t> aux;
+    std::vector<cudaEvent_t> fj;
+    size_t fj_next = 0;
+
+    cudaError_t aux_stream(size_t k, cudaStream_t* out) {
+        while (aux.size() <= k) {
+            cudaStream_t st;
+            RB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            aux.push_back(st);
+        }
+        *out = aux[k];
+        return cudaSuccess;
+    }
+    // `to` waits for everything enqueued on `from` so far
+    cudaError_t order_after(cudaStream_t from, cudaStream_t to) {
+        if (fj_next == fj.size()) {
+            cudaEvent_t ev;
+            RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            fj.push_back(ev);
+        }
+        cudaEvent_t ev = fj[fj_next++];
+        RB_CUDA_TRY(cudaEventRecord(ev, from));
+        return cudaStreamWaitEvent(to, ev, 0);
+    }
+
+    // One op_steps block of every instance.  The QUBO steps and the JRP steps
+    // are independent chains (separate branches of the graph), and within a
+    // JRP half-step the x shared-memory classes and the y/z cluster-size
+    // groups run side by side; the gather of all control blocks joins them.
     cudaError_t enqueue_block() {
         const int gq = sms * shapes.grid_mult;
-        const bool hq = !q.empty(), hj = !j.empty();
+        // only the kinds with running instances (a retired kind leaves the graph)
+        const bool hq = graph_q, hj = graph_j;
         long long nodes = 0;
-        for (int s = 0; s < op_steps; ++s) {
-            const bool last = s + 1 == op_steps;
-            if (hq) {
-                if (last) {
-                    bq_node<Real, true, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
-                    bq_edge<Real, true, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
+        fj_next = 0;
+        cudaStream_t sq = stream;
+        if (hq && hj) {
+            RB_CUDA_TRY(aux_stream(0, &sq));
+            RB_CUDA_TRY(order_after(stream, sq));
+        }
+        if (hq) {
+            for (int s = 0; s < op_steps; ++s) {
+                if (s + 1 == op_steps) {
+                    bq_node<Real, true, true><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
+                    bq_edge<Real, true, true><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
                 } else {
-                    bq_node<Real, true, false><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
-                    bq_edge<Real, true, false><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
+                    bq_node<Real, true, false><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, s, 0);
+                    bq_edge<Real, true, false><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, s, 0);
                 }
                 nodes += 2;
             }
-            if (hj) {
-                RB_CUDA_TRY((last ? launch_x<true, true>(s, 0) : launch_x<true, false>(s, 0)));
-                nodes += 1;
-                for (int c = 1; c < kMaxGroups; ++c) {
-                    if (!groups[c]) continue;
-                    RB_CUDA_TRY((last ? launch_yz<true, true>(c, s, 0) : launch_yz<true, false>(c, s, 0)));
-                    nodes += 1;
-                }
-            }
-        }
-        if (hq) {
-            bq_lower<Real><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_qlow.buf.ptr, counts.ptr + kQLow);
-            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, stream>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
-                                                                     counts.ptr + kQCheck, 1);
-            bq_node<Real, false, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, 0, 1);
-            bq_edge<Real, false, true><<<gq, praq::kBlock, 0, stream>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, 0, 1);
-            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, stream>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
-                                                                     counts.ptr + kQCheck, 2);
+            bq_lower<Real><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_qlow.buf.ptr, counts.ptr + kQLow);
+            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, sq>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
+                                                                 counts.ptr + kQCheck, 1);
+            bq_node<Real, false, true><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_node.buf.ptr, counts.ptr + kNode, 0, 1);
+            bq_edge<Real, false, true><<<gq, praq::kBlock, 0, sq>>>(qdevs.buf.ptr, t_edge.buf.ptr, counts.ptr + kEdge, 0, 1);
+            bq_check<Real><<<sms * 4, praq::kCheckBlock, 0, sq>>>(qdevs.buf.ptr, qmeta.buf.ptr, l_qcheck.buf.ptr,
+                                                                 counts.ptr + kQCheck, 2);
             nodes += 5;
         }
         if (hj) {
+            // the x classes of one half-step, side by side
+            auto x_stage = [&](auto launch_one) -> cudaError_t {
+                size_t k = 1;
+                bool first = true;
+                for (int c = 0; c < kXClasses; ++c) {
+                    if (!xclasses[c]) continue;
+                    cudaStream_t st = stream;
+                    if (!first) {
+                        RB_CUDA_TRY(aux_stream(k++, &st));
+                        RB_CUDA_TRY(order_after(stream, st));
+                    }
+                    RB_CUDA_TRY(launch_one(c, st));
+                    ++nodes;
+                    first = false;
+                }
+                for (size_t a = 1; a < k; ++a) RB_CUDA_TRY(order_after(aux[a], stream));
+                return cudaSuccess;
+            };
+            // the y half-step beside the z cluster-size groups
+            auto yz_stage = [&](auto launch_y_one, auto launch_one) -> cudaError_t {
+                size_t k = 1;
+                int zgroup[kMaxGroups];
+                int nz = 0;
+                for (int c = 1; c < kMaxGroups; ++c) {   // fork every z group off the main stream first
+                    if (!groups[c]) continue;
+                    cudaStream_t st;
+                    RB_CUDA_TRY(aux_stream(k++, &st));
+                    RB_CUDA_TRY(order_after(stream, st));
+                    zgroup[nz++] = c;
+                }
+                RB_CUDA_TRY(launch_y_one(stream));
+                ++nodes;
+                for (int g = 0; g < nz; ++g) {
+                    RB_CUDA_TRY(launch_one(zgroup[g], aux[size_t(g) + 1]));
+                    ++nodes;
+                }
+                for (size_t a = 1; a < k; ++a) RB_CUDA_TRY(order_after(aux[a], stream));
+                return cudaSuccess;
+            };
+            for (int s = 0; s < op_steps; ++s) {
+                const bool last = s + 1 == op_steps;
+                RB_CUDA_TRY(x_stage([&](int c, cudaStream_t st) {
+                    return last ? launch_x<true, true>(c, s, 0, st) : launch_x<true, false>(c, s, 0, st);
+                }));
+                RB_CUDA_TRY(yz_stage(
+                    [&](cudaStream_t st) { return last ? launch_y<true, true>(s, 0, st) : launch_y<true, false>(s, 0, st); },
+                    [&](int c, cudaStream_t st) {
+                        return last ? launch_yz<true, true>(c, s, 0, st) : launch_yz<true, false>(c, s, 0, st);
+                    }));
+            }
             bj_upper<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_up.buf.ptr, counts.ptr + kUp);
             bj_lower<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_jlow.buf.ptr, counts.ptr + kJLow);
             bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
                                                                      counts.ptr + kJCheck, 1);
-            RB_CUDA_TRY((launch_x<false, true>(0, 1)));
-            nodes += 4;
-            for (int c = 1; c < kMaxGroups; ++c) {
-                if (!groups[c]) continue;
-                RB_CUDA_TRY((launch_yz<false, true>(c, 0, 1)));
-                nodes += 1;
-            }
+            nodes += 3;
+            RB_CUDA_TRY(x_stage([&](int c, cudaStream_t st) { return launch_x<false, true>(c, 0, 1, st); }));
+            RB_CUDA_TRY(yz_stage([&](cudaStream_t st) { return launch_y<false, true>(0, 1, st); },
+                                 [&](int c, cudaStream_t st) { return launch_yz<false, true>(c, 0, 1, st); }));
             bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
                                                                      counts.ptr + kJCheck, 2);
             nodes += 1;
         }
+        if (hq && hj) RB_CUDA_TRY(order_after(sq, stream));
         const int slots = int(q.size() + j.size());
         b_gather<Real><<<std::max(1, ceil_div(slots, 128)), 128, 0, stream>>>(
             qdevs.buf.ptr, int(q.size()), jdevs.buf.ptr, int(j.size()), live.buf.ptr, summary.ptr);
@@ -638,6 +777,19 @@ struct Engine final : EngineBase {
         exec = nullptr;
         graph = nullptr;
         if (set_attributes()) return -int(cudaErrorUnknown);
+        // every auxiliary stream and fork/join event exists before the capture
+        int ex = 0, eg = 0;
+        for (bool b : xclasses) ex += b;
+        for (bool b : groups) eg += b;
+        const size_t wide = size_t(std::max(ex, eg)) + 1;
+        const size_t events_needed = 2 + size_t(op_steps + 1) * 2 * size_t(std::max(0, ex - 1) + eg);
+        cudaStream_t tmp;
+        if (aux_stream(wide, &tmp)) return -int(cudaErrorUnknown);
+        while (fj.size() < events_needed) {
+            cudaEvent_t ev;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) return -int(cudaErrorUnknown);
+            fj.push_back(ev);
+        }
         if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) return -int(cudaErrorUnknown);
         const cudaError_t st = enqueue_block();
         const cudaError_t st2 = cudaStreamEndCapture(stream, &graph);

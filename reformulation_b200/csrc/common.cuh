@@ -5,6 +5,8 @@
 // on the launch shape only, so a solve is bitwise reproducible run to run).
 #pragma once
 
+#include <utility>
+
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -66,6 +68,33 @@ __device__ __forceinline__ void reduce_rows(const double* rows, int count, doubl
         for (int k = 0; k < K; ++k) v[k] += rows[size_t(r) * K + k];
     }
     block_sums<K>(v, scratch, out);
+}
+
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may start before the kernel ahead of it on
+// the stream has finished.  pdl_wait() blocks until that kernel has completed
+// and its memory is visible (a no-op for a kernel launched without the
+// attribute); pdl_launch_dependents() lets the next kernel start its CTAs as
+// soon as every CTA of this one has issued it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+// Launch `kernel` on `stream` with the programmatic stream-serialization
+// attribute (the kernel must call pdl_wait() before it touches memory the
+// previous kernel writes).
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t stream, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 template <class T>

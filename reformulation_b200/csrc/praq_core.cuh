@@ -112,7 +112,7 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
 }
 
 #ifndef RB200_PRAQ_STAGE
-#define RB200_PRAQ_STAGE 256   // compile-time tunable (sweeps build with -D)
+#define RB200_PRAQ_STAGE 512   // compile-time tunable (sweeps build with -D)
 #endif
 constexpr int kStage = RB200_PRAQ_STAGE;   // half-edge values a warp stages per pass
 
@@ -221,6 +221,8 @@ template <class Real, bool Reflect, bool Check>
 __global__ void __launch_bounds__(kBlock)
 node_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
             int bounds_at_1, int gate) {
+    pdl_wait();
+    pdl_launch_dependents();
     node_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ys, yc, step, bounds_at_1, gate);
 }
 
@@ -302,6 +304,8 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
 template <class Real, bool Reflect, bool Check>
 __global__ void __launch_bounds__(kBlock)
 edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) {
+    pdl_wait();
+    pdl_launch_dependents();
     edge_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ysrc, step, bounds_at_1, gate);
 }
 
@@ -328,6 +332,8 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
 template <class Real>
 __global__ void __launch_bounds__(kBlock)
 lower_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc) {
+    pdl_wait();
+    pdl_launch_dependents();
     lower_kernel_tile<Real>(d, blockIdx.x, ys, yc);
 }
 
@@ -412,6 +418,8 @@ __global__ void __launch_bounds__(kCheckBlock)
 check_kernel(Control* c, Params p, const double* __restrict__ scale_ptr,
              const double* __restrict__ pnode, int nbn, const double* __restrict__ pedge, int nbe,
              const double* __restrict__ plower, int nbl, int mode) {
+    pdl_wait();
+    pdl_launch_dependents();
     check_body(c, p, scale_ptr, pnode, nbn, pedge, nbe, plower, nbl, mode);
 }
 
@@ -792,19 +800,19 @@ struct Solver final : SolverBase {
         const int op = int(p.op_steps);
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
-                RB_TIMED(0, (node_kernel<Real, true, false><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, s, 0, 0)));
-                if (m) RB_TIMED(1, (edge_kernel<Real, true, false><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
+                RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
+                if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, false>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             } else {
-                RB_TIMED(2, (node_kernel<Real, true, true><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, s, 0, 0)));
-                if (m) RB_TIMED(3, (edge_kernel<Real, true, true><<<nb_edge, kBlock, 0, stream>>>(d, nullptr, s, 0, 0)));
+                RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
+                if (m) RB_TIMED(3, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, true>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             }
         }
-        RB_TIMED(4, (lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, d.u2c)));
-        RB_TIMED(5, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node,
+        RB_TIMED(4, RB_CUDA_TRY(launch_pdl(lower_kernel<Real>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c)));
+        RB_TIMED(5, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 1)));
-        RB_TIMED(6, (node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.u2s, d.u2c, 0, 0, 1)));
-        if (m) RB_TIMED(7, (edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.u2s, 0, 0, 1)));
-        RB_TIMED(8, (check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node,
+        RB_TIMED(6, RB_CUDA_TRY(launch_pdl(node_kernel<Real, false, true>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c, 0, 0, 1)));
+        if (m) RB_TIMED(7, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, false, true>, nb_edge, kBlock, stream, d, (const Real*)d.u2s, 0, 0, 1)));
+        RB_TIMED(8, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 2)));
         RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
         return cudaGetLastError();

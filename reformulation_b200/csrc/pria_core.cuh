@@ -65,7 +65,9 @@ constexpr int kXTile = 16;              // columns per tile of the x half-step (
 constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
 constexpr int kMaxCluster = 16;
 constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
-constexpr int kZUnroll = 4;          // z elements per thread in flight (y/z kernel)
+constexpr int kZUnroll = 8;          // z elements per thread in flight (z kernel)
+constexpr int kYThreads = 256;       // y kernel: one warp per row, kYThreads / 32 rows per tile
+constexpr int kZThreads = 512;       // z kernel CTA
 
 struct Control {
     double omega, theta, fp_error, check_error;
@@ -106,7 +108,7 @@ struct Dev {
     Real k0;                 // K0 / scale
     Real *xh, *x0, *r, *yh, *y0, *zh, *z0;   // combined point (next step), anchors, reflection
     Real *x2s, *dxs, *y2s, *z2s;             // at checks: the step and x1 - x2
-    double *px, *pyz, *pup, *plo;            // partial rows
+    double *px, *py, *pyz, *pup, *plo;       // partial rows (pyz: the z half-step's)
     double *thx, *thy, *thz;                 // last thresholds: per column, row, block
     Control* ctl;
 };
@@ -331,51 +333,44 @@ x_kernel(Dev<Real> d, const Real* xsrc, const Real* __restrict__ ysrc, const Rea
     x_kernel_tile<Real, TW, Reflect, Check>(d, blockIdx.x, xsrc, ysrc, zsrc, step, gate);
 }
 
-// y and z half-steps (solver.py:421-423) for period block s, one cluster of
-// `csize` CTAs per block; CTA `rank` owns rows [r0, r1) of the block.
-template <class Real, int kThreads, bool Reflect, bool Check>
-__device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* ysrc, const Real* zsrc, int step, int gate) {
+// y half-step (solver.py:421-422) for one tile of rows: warp w takes row
+// g = tile * (rows per tile) + w of the period-major order (block s, item i),
+// a contiguous run of Tp - s values.  y' = P_Y(y + r) onto the K_i simplex
+// (Michelot over the row staged in the warp's slice of shared memory,
+// warm-started from the row's last threshold), the next combined y, and at
+// checks y2 and the y parts of the check sums.  `rows` holds
+// (threads / 32) * row_cap reals, row_cap >= Tp.
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void y_kernel_tile(const Dev<Real>& d, int tile, const Real* ysrc, int step, int gate,
+                                              Real* rows, int row_cap) {
     const Control* c = d.ctl;
-    if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
-    cg::cluster_group cluster = cg::this_cluster();
-    const int csize = d.csize;
-    const int rank = int(cluster.block_rank());
-    const int len = d.tp - s;
-    const long long base = blk(d.n, d.tp, s);
-    const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real* vz = reinterpret_cast<Real*>(smem_raw);
-    __shared__ double part[2][2];
+    if (skip(c, gate)) return;
     __shared__ double scratch[3 * 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Real* v = rows + size_t(warp) * row_cap;
+    const long long g = (long long)tile * (blockDim.x >> 5) + warp;
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
-    const bool vanilla = !Reflect && (gate & kGateVanilla);   // as in the x half-step
+    // Without Reflect: a vanilla step (next = the step, anchor kept) or the
+    // step that makes the current point the anchor (drift against the old one)
+    const bool vanilla = !Reflect && (gate & kGateVanilla);
     const bool drift = Reflect || (gate & kGateDrift);
-    double acc[3] = {0.0, 0.0, 0.0};   // |dy|^2 + |dz|^2, <dx, dy + dz>, drift
-
-    // phase A: y rows, and the z values into shared memory
-    for (int i = r0 + warp; i < r1; i += nwarps) {
-        const long long e0 = base + (long long)i * len;
-        Real v[32];
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const int q = lane + 32 * k;
-            if (q < len) {
-                const Real rr = d.r[e0 + q];
-                v[k] = ysrc[e0 + q] + rr;
-                vz[(i - r0) * len + q] = zsrc[e0 + q] + rr;
-            }
-        }
+    double acc[3] = {0.0, 0.0, 0.0};   // |dy|^2, <dx, dy>, drift
+    if (g < (long long)d.tp * d.n) {    // uniform over the warp
+        const int s = int(g / d.n), i = int(g - (long long)s * d.n);
+        const int len = d.tp - s;
+        const long long e0 = blk(d.n, d.tp, s) + (long long)i * len;
+#pragma unroll 8
+        for (int q = lane; q < len; q += 32) v[q] = ysrc[e0 + q] + d.r[e0 + q];
+        __syncwarp();
         double* slot = d.thy + (long long)s * d.n + i;
-        const double th = michelot_regs(v, len, double(d.k[i]), *slot);
+        const double th = michelot_smem(v, len, double(d.k[i]), *slot);
         if (lane == 0) *slot = th;
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const int q = lane + 32 * k;
-            if (q < len) {
+#pragma unroll 4
+        for (int q = lane; q < len; q += 32) {
+            {
                 const long long e = e0 + q;
-                const Real y2 = Real(fmax(double(v[k]) - th, 0.0));
+                const Real y2 = Real(fmax(double(v[q]) - th, 0.0));
                 const Real y1 = ysrc[e];
                 const Real yd = drift ? d.y0[e] : y1;
                 const Real ya = Reflect ? yd : y1;
@@ -391,6 +386,64 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
             }
         }
     }
+    if (Check) {
+        block_sums<3>(acc, scratch, acc);
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 3; ++k) d.py[size_t(tile) * 3 + k] = acc[k];
+    }
+}
+
+template <class Real, bool Reflect, bool Check>
+__global__ void __launch_bounds__(kYThreads)
+y_kernel(Dev<Real> d, const Real* ysrc, int step, int gate) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    y_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ysrc, step, gate, reinterpret_cast<Real*>(smem_raw), d.tp);
+}
+
+// z half-step (solver.py:423) for period block s, one cluster of `csize` CTAs
+// per block; CTA `rank` owns rows [r0, r1) of the block, a contiguous slice.
+// z + r of the slice goes to shared memory, the threshold of the whole block
+// comes from Michelot rounds whose (sum, count) pass through distributed
+// shared memory, then the slice's z is written.
+template <class Real, int kThreads, bool Reflect, bool Check>
+__device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zsrc, int step, int gate) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
+    cg::cluster_group cluster = cg::this_cluster();
+    const int csize = d.csize;
+    const int rank = int(cluster.block_rank());
+    const int len = d.tp - s;
+    const long long base = blk(d.n, d.tp, s);
+    const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* vz = reinterpret_cast<Real*>(smem_raw);
+    __shared__ double part[2][2];
+    __shared__ double scratch[3 * 32];
+    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
+    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    const bool vanilla = !Reflect && (gate & kGateVanilla);   // as in the y half-step
+    const bool drift = Reflect || (gate & kGateDrift);
+    double acc[3] = {0.0, 0.0, 0.0};   // |dz|^2, <dx, dz>, drift
+    const int mine = (r1 - r0) * len;
+    const long long sbase = base + (long long)r0 * len;
+
+    // phase A: z + r of the slice into shared memory, kZUnroll loads in flight
+    for (int qb = threadIdx.x; qb < mine; qb += kThreads * kZUnroll) {
+        Real zv[kZUnroll], rv[kZUnroll];
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q < mine) {
+                zv[u] = zsrc[sbase + q];
+                rv[u] = d.r[sbase + q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kZUnroll; ++u) {
+            const int q = qb + u * kThreads;
+            if (q < mine) vz[q] = zv[u] + rv[u];
+        }
+    }
     __syncthreads();
 
     // phase B: the z threshold over the whole block, across the cluster.
@@ -398,7 +451,6 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
     // cluster barrier every CTA adds all ranks' partials in rank order, so
     // every CTA takes the same decisions.  The two parities let a round write
     // its partials while no CTA can still be reading that buffer.
-    const int mine = (r1 - r0) * len;
     int parity = 0;
     auto active = [&](double th, double& S, int& C) {
         double b[2] = {0.0, 0.0};
@@ -430,7 +482,6 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
     if (rank == 0 && threadIdx.x == 0) d.thz[s] = thz;
 
     // phase C: z
-    const long long sbase = base + (long long)r0 * len;
     for (int qb = threadIdx.x; qb < mine; qb += kThreads * kZUnroll) {
         Real z1v[kZUnroll], zav[kZUnroll], dxv[kZUnroll];
 #pragma unroll
@@ -470,8 +521,8 @@ __device__ __forceinline__ void yz_task(const Dev<Real>& d, int s, const Real* y
 
 template <class Real, int kThreads, bool Reflect, bool Check>
 __global__ void __launch_bounds__(kThreads)
-yz_kernel(Dev<Real> d, const Real* ysrc, const Real* zsrc, int step, int gate) {
-    yz_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, ysrc, zsrc, step, gate);
+z_kernel(Dev<Real> d, const Real* zsrc, int step, int gate) {
+    z_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
 }
 
 // The primal bound terms at x for period block s (solver.py:347-365):
@@ -582,15 +633,18 @@ __device__ __forceinline__ bool should_stop(double gap, long long iteration, con
 // ends the vanilla phase and starts the Halpern one (the primal weight from
 // the drift of the vanilla phase, solver.py:680-694).
 __device__ __forceinline__ void check_body(Control* c, Params p, const double* __restrict__ px, int nbx,
-             const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
-             const double* __restrict__ plo, int nblo, int mode) {
+             const double* __restrict__ py, int nby, const double* __restrict__ pyz, int nbyz,
+             const double* __restrict__ pup, int nbup, const double* __restrict__ plo, int nblo, int mode) {
     if (c->terminated) return;
     if (mode == 2 && !c->restart) return;
     __shared__ double scratch[3 * 32];
-    __shared__ double xs[2], yzs[3], up[3], lo[1];
+    __shared__ double xs[2], yzs[3], ys_[3], up[3], lo[1];
     if (mode != 3) {
         reduce_rows<2>(px, nbx, scratch, xs);
+        reduce_rows<3>(py, nby, scratch, ys_);
         reduce_rows<3>(pyz, nbyz, scratch, yzs);
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 3; ++k) yzs[k] += ys_[k];   // y parts + z parts, in that order
     }
     if (mode != 2 && mode != 4) {
         reduce_rows<3>(pup, nbup, scratch, up);
@@ -684,9 +738,10 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* _
 
 __global__ void __launch_bounds__(kCheckBlock)
 check_kernel(Control* c, Params p, const double* __restrict__ px, int nbx,
+             const double* __restrict__ py, int nby,
              const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
              const double* __restrict__ plo, int nblo, int mode) {
-    check_body(c, p, px, nbx, pyz, nbyz, pup, nbup, plo, nblo, mode);
+    check_body(c, p, px, nbx, py, nby, pyz, nbyz, pup, nbup, plo, nblo, mode);
 }
 
 // The start point: the projection of zero, i.e. each simplex's centre:
@@ -940,20 +995,22 @@ struct Solver final : SolverBase {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     PoolBuf<Real> h, k, xh, x0, r, yh, y0, zh, z0, x2s, dxs, y2s, z2s;
-    PoolBuf<double> px, pyz, pup, plo, final_up, thx, thy, thz;
+    PoolBuf<double> px, py, pyz, pup, plo, final_up, thx, thy, thz;
     PoolBuf<double> warm[3];   // dense warm start (FP64), optional
     bool has_warm = false;
     PoolBuf<Control> ctl;
     Control* mirror = nullptr;
     Dev<Real> d{};
-    int tw = kXTile, nbx = 1, nbyz = 1, nblo = 1;
+    int tw = kXTile, nbx = 1, nby = 1, nbyz = 1, nblo = 1;
     size_t x_smem = 0, yz_smem = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
-    static constexpr int kYZThreads = 256;
+    static constexpr int kZThreadsPerCta = kZThreads;
+    // y rows: one padded row of at most kMaxPeriods reals per warp
+    static constexpr size_t y_smem_limit() { return size_t(kYThreads / 32) * kMaxPeriods * sizeof(Real); }
     // x tiles: kXTile columns of a padded row of at most kMaxPeriods (+1)
     // FP64 values
     static constexpr size_t x_smem_limit() {
@@ -967,7 +1024,7 @@ struct Solver final : SolverBase {
         for (auto& ev : done) if (ev) cudaEventDestroy(ev);
         for (auto& ev : evpool) cudaEventDestroy(ev);
         for (auto* b : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s}) b->release();
-        for (auto* b : {&px, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
+        for (auto* b : {&px, &py, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
         for (auto& b : warm) b.release();
         ctl.release();
         if (stream) cudaStreamSynchronize(stream);
@@ -1075,8 +1132,10 @@ struct Solver final : SolverBase {
         yz_smem = size_t((n + csize - 1) / csize) * tp * sizeof(Real);
         if (yz_smem > size_t(kSliceBytes)) return cudaErrorInvalidValue;
         nbyz = tp * csize;
+        nby = int(((long long)tp * n + kYThreads / 32 - 1) / (kYThreads / 32));
         RB_CUDA_TRY(px.alloc(size_t(nbx) * 2, stream));
         RB_CUDA_TRY(pyz.alloc(size_t(nbyz) * 3, stream));
+        RB_CUDA_TRY(py.alloc(size_t(nby) * 3, stream));
         RB_CUDA_TRY(pup.alloc(size_t(tp) * 3, stream));
         RB_CUDA_TRY(plo.alloc(size_t(nblo), stream));
         RB_CUDA_TRY(final_up.alloc(size_t(tp) * 3, stream));
@@ -1092,7 +1151,7 @@ struct Solver final : SolverBase {
         d.h = h.ptr;
         d.xh = xh.ptr; d.x0 = x0.ptr; d.r = r.ptr; d.yh = yh.ptr; d.y0 = y0.ptr; d.zh = zh.ptr; d.z0 = z0.ptr;
         d.x2s = x2s.ptr; d.dxs = dxs.ptr; d.y2s = y2s.ptr; d.z2s = z2s.ptr;
-        d.px = px.ptr; d.pyz = pyz.ptr; d.pup = pup.ptr; d.plo = plo.ptr; d.ctl = ctl.ptr;
+        d.px = px.ptr; d.py = py.ptr; d.pyz = pyz.ptr; d.pup = pup.ptr; d.plo = plo.ptr; d.ctl = ctl.ptr;
         d.thx = thx.ptr; d.thy = thy.ptr; d.thz = thz.ptr;
         prm.tolerance = p.tolerance;
         prm.eta = p.eta;
@@ -1108,7 +1167,7 @@ struct Solver final : SolverBase {
         prm.omega0 = p.omega;
         prm.vanilla_solve = p.use_halpern ? 0 : 1;
         RB_CUDA_TRY(set_attributes());
-        block_nodes = 2LL * p.op_steps + 3 + 3;
+        block_nodes = 3LL * p.op_steps + 3 + 4;   // x, y, z per step; bounds, check; restart x, y, z, check
         return cudaGetLastError();
     }
 
@@ -1124,7 +1183,9 @@ struct Solver final : SolverBase {
     }
     template <bool R, bool C>
     cudaError_t yz_attr() {
-        auto fn = yz_kernel<Real, kYZThreads, R, C>;
+        RB_CUDA_TRY(cudaFuncSetAttribute(y_kernel<Real, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(y_smem_limit())));
+        auto fn = z_kernel<Real, kZThreads, R, C>;
         RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
         RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         return cudaSuccess;
@@ -1157,10 +1218,14 @@ struct Solver final : SolverBase {
     }
 
     template <bool R, bool C>
+    // the y half-step (one warp per row) and then the z half-step (a cluster
+    // per period block); two launches
     cudaError_t launch_yz(const Real* ys, const Real* zs, int step, int gate) {
+        y_kernel<Real, R, C><<<nby, kYThreads, size_t(kYThreads / 32) * tp * sizeof(Real), stream>>>(d, ys, step, gate);
+        RB_CUDA_TRY(cudaGetLastError());
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(unsigned(tp * d.csize));
-        cfg.blockDim = dim3(kYZThreads);
+        cfg.blockDim = dim3(kZThreads);
         cfg.dynamicSmemBytes = yz_smem;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
@@ -1170,11 +1235,11 @@ struct Solver final : SolverBase {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, yz_kernel<Real, kYZThreads, R, C>, d, ys, zs, step, gate);
+        return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C>, d, zs, step, gate);
     }
 
     cudaError_t launch_check(int mode) {
-        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.px, nbx, d.pyz, nbyz, d.pup, tp, d.plo,
+        check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.px, nbx, d.py, nby, d.pyz, nbyz, d.pup, tp, d.plo,
                                                    nblo, mode);
         return cudaGetLastError();
     }
@@ -1275,7 +1340,7 @@ struct Solver final : SolverBase {
         RB_CUDA_TRY((launch_yz<false, true>(d.y0, d.z0, 0, 0)));
         RB_CUDA_TRY(launch_check(0));
         RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
-        nlaunch += 5;
+        nlaunch += 6;
         return cudaStreamSynchronize(stream);
     }
 
@@ -1289,7 +1354,7 @@ struct Solver final : SolverBase {
         upper_kernel<Real><<<tp, kAuxThreads, 0, stream>>>(d, d.xh, tp, 0);
         lower_kernel<Real><<<nblo, kAuxThreads, 0, stream>>>(d, d.yh, d.zh);
         RB_CUDA_TRY(launch_check(3));
-        nlaunch += 2LL * p.op_steps + 3;
+        nlaunch += 3LL * p.op_steps + 3;
         return cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
     }
 
@@ -1313,7 +1378,7 @@ struct Solver final : SolverBase {
         RB_CUDA_TRY((launch_x<false, true>(d.xh, d.yh, d.zh, 0, kGateDrift)));
         RB_CUDA_TRY((launch_yz<false, true>(d.yh, d.zh, 0, kGateDrift)));
         RB_CUDA_TRY(launch_check(4));
-        nlaunch += 3;
+        nlaunch += 4;
         RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
         return cudaStreamSynchronize(stream);
     }
@@ -1448,7 +1513,7 @@ struct Solver final : SolverBase {
         size_t b = 0;
         for (auto* x : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s})
             b += x->count * sizeof(Real);
-        for (auto* x : {&px, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b += x->count * sizeof(double);
+        for (auto* x : {&px, &py, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b += x->count * sizeof(double);
         return b + sizeof(Control);
     }
 };
