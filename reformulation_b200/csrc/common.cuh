@@ -97,6 +97,12 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, cud
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+// Start bringing the line of `p` into L2 (no register, no wait): for data a
+// later pass of the same thread block reads, so that pass finds it on chip.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) {
     return v < lo ? lo : (v > hi ? hi : v);

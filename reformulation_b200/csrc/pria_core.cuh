@@ -61,7 +61,10 @@ constexpr int kXThreads = 256;
 constexpr int kAuxThreads = 256;
 constexpr int kCheckBlock = 256;
 constexpr int kLowTW = 32;              // columns per tile of the lower-bound pass
-constexpr int kXTile = 16;              // columns per tile of the x half-step (FP64 tile)
+#ifndef RB200_PRIA_XTILE
+#define RB200_PRIA_XTILE 8              // compile-time tunable (sweeps build with -D)
+#endif
+constexpr int kXTile = RB200_PRIA_XTILE;   // columns per tile of the x half-step (FP64 tile)
 constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
 constexpr int kMaxCluster = 16;
 constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
@@ -101,6 +104,9 @@ __host__ __device__ __forceinline__ long long blk(int n, int tp, int s) {
 template <class Real>
 struct Dev {
     int n, t, tp, ntc, ntc_low, csize;
+    int zstaged;             // 1: z + r of a block sits in its cluster's shared memory;
+                             // 0: too large for that, every Michelot round recomputes
+                             //    it from global memory (L2-resident)
     long long nd;
     double eta;
     const Real* h;           // [nd] holding costs / scale
@@ -258,6 +264,8 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
                 hv[u] = d.h[ev[u]];
                 yv[u] = ysrc[ev[u]];
                 zv[u] = zsrc[ev[u]];
+                // the anchor the second pass reads, on chip by then
+                if ((Reflect || (gate & kGateDrift)) && ((col & 7) == 0 || tt == s)) prefetch_l2(d.x0 + ev[u]);
             }
         }
 #pragma unroll
@@ -361,7 +369,11 @@ __device__ __forceinline__ void y_kernel_tile(const Dev<Real>& d, int tile, cons
         const int len = d.tp - s;
         const long long e0 = blk(d.n, d.tp, s) + (long long)i * len;
 #pragma unroll 8
-        for (int q = lane; q < len; q += 32) v[q] = ysrc[e0 + q] + d.r[e0 + q];
+        for (int q = lane; q < len; q += 32) {
+            v[q] = ysrc[e0 + q] + d.r[e0 + q];
+            if (drift && (q & 7) == 0) prefetch_l2(d.y0 + e0 + q);   // one per 32-byte sector
+            if (Check && (q & 7) == 0) prefetch_l2(d.dxs + e0 + q);
+        }
         __syncwarp();
         double* slot = d.thy + (long long)s * d.n + i;
         const double th = michelot_smem(v, len, double(d.k[i]), *slot);
@@ -427,8 +439,12 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
     const int mine = (r1 - r0) * len;
     const long long sbase = base + (long long)r0 * len;
 
+    const bool staged = d.zstaged != 0;
+    // v(q) = z + r of the slice's element q, in the same arithmetic either way
+    auto vval = [&](int q) -> Real { return staged ? vz[q] : Real(zsrc[sbase + q] + d.r[sbase + q]); };
+
     // phase A: z + r of the slice into shared memory, kZUnroll loads in flight
-    for (int qb = threadIdx.x; qb < mine; qb += kThreads * kZUnroll) {
+    for (int qb = threadIdx.x; staged && qb < mine; qb += kThreads * kZUnroll) {
         Real zv[kZUnroll], rv[kZUnroll];
 #pragma unroll
         for (int u = 0; u < kZUnroll; ++u) {
@@ -436,6 +452,8 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
             if (q < mine) {
                 zv[u] = zsrc[sbase + q];
                 rv[u] = d.r[sbase + q];
+                if (drift && (q & 7) == 0) prefetch_l2(d.z0 + sbase + q);
+                if (Check && (q & 7) == 0) prefetch_l2(d.dxs + sbase + q);
             }
         }
 #pragma unroll
@@ -455,7 +473,7 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
     auto active = [&](double th, double& S, int& C) {
         double b[2] = {0.0, 0.0};
         for (int q = threadIdx.x; q < mine; q += kThreads) {
-            const double x = double(vz[q]);
+            const double x = double(vval(q));
             if (th == -INFINITY || x > th) {
                 b[0] += x;
                 b[1] += 1.0;
@@ -498,7 +516,7 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
             const int q = qb + u * kThreads;
             if (q >= mine) continue;
             const long long e = sbase + q;
-            const Real z2 = Real(fmax(double(vz[q]) - thz, 0.0));
+            const Real z2 = Real(fmax(double(vval(q)) - thz, 0.0));
             const Real z1 = z1v[u], za = Reflect ? zav[u] : z1;
             d.zh[e] = vanilla ? z2 : lwn * (Real(2) * z2 - z1) + rwn * za;
             if (!Reflect && !vanilla) d.z0[e] = z1;
@@ -1130,7 +1148,11 @@ struct Solver final : SolverBase {
             ++csize;
         if (csize > n) csize = n;
         yz_smem = size_t((n + csize - 1) / csize) * tp * sizeof(Real);
-        if (yz_smem > size_t(kSliceBytes)) return cudaErrorInvalidValue;
+        d.zstaged = 1;
+        if (yz_smem > size_t(kSliceBytes)) {   // the largest block exceeds a full cluster's slices
+            d.zstaged = 0;
+            yz_smem = 0;
+        }
         nbyz = tp * csize;
         nby = int(((long long)tp * n + kYThreads / 32 - 1) / (kYThreads / 32));
         RB_CUDA_TRY(px.alloc(size_t(nbx) * 2, stream));

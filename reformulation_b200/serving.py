@@ -85,6 +85,7 @@ class Server:
     tolerance: float = 1e-4
     max_iter: int = 200_000
     blocks_in_flight: int = 2
+    admit_every: int = 4          # blocks between admissions while instances run
     batch: Batch | EscalatingBatch = field(init=False)
     waiting: deque = field(default_factory=deque)
     running: dict = field(default_factory=dict)   # engine id -> (Request, admitted time)
@@ -143,12 +144,16 @@ class Server:
         them; returns the completions in finishing order."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         t0 = time.perf_counter() if t0 is None else t0
+        since_admit = self.admit_every
         while pending or self.waiting or self.running:
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 self.submit(pending.popleft())
-            # the engine drains before it lays out newcomers, so retire first
-            if self.waiting:
+            # the engine drains before it lays out newcomers, so retire first;
+            # while instances run, newcomers are admitted every `admit_every`
+            # blocks (each admission empties the pipeline once)
+            if self.waiting and (not self.running or since_admit >= self.admit_every):
+                since_admit = 0
                 while self.batch.inflight():
                     _, ids = self.batch.sync()
                     for eid in ids:
@@ -161,6 +166,7 @@ class Server:
             while self.batch.inflight() < self.blocks_in_flight:
                 self.batch.launch()
             _, ids = self.batch.sync()
+            since_admit += 1
             for eid in ids:
                 self._finish(eid, t0)
             # an instance that terminated at its cold start never enters a block

@@ -222,3 +222,23 @@ def test_vanilla_and_warm_phase_match_reference(lib, oracle_lib, mode):
                         **{k: v for k, v in mode.items() if k not in ("max_iter", "tolerance")})
     m = lib.solve(inst, pm, precision="mixed")
     assert m.status == 0 and rel(m.primal_objective, s.primal_objective) <= 1e-3
+
+
+def test_block_beyond_cluster_shared_memory(native):
+    """A period block larger than a full cluster's shared-memory slices (FP64,
+    N T above 196,608) takes the z half-step that recomputes z + r from global
+    memory each Michelot round; it runs and agrees with the staged FP32 solve
+    of the same instance to FP32 accuracy after the same iterations."""
+    from reformulation_b200 import pria
+    inst = jrp_demand(40, 400, 500)
+    p = pria.Library().parameters(48, 1e-12)
+    with pria.DeviceSolver(inst, p, "fp64") as a:
+        assert a.run() == 0
+        ra = a.result()
+    with pria.DeviceSolver(inst, p, "mixed") as b:
+        assert b.run() == 0
+        rb = b.result()
+    assert ra.iterations == rb.iterations == 48
+    assert ra.dual_objective <= ra.primal_objective
+    assert rel(ra.primal_objective, rb.primal_objective) <= 1e-3
+    assert rel(ra.dual_objective, rb.dual_objective) <= 1e-3
