@@ -225,32 +225,20 @@ def time_solves(dev, steps, flush, torch, stream):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
     from reformulation_b200 import build as native_build
     from reformulation_b200 import praq
     from reformulation_b200.instances import qubo_uniform_edges
 
+    from reformulation_b200.replicas import Replicas
+
     world, rank, local = dist_setup()
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
-                                timeout=__import__("datetime").timedelta(seconds=300))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    rep = Replicas("nccl", device=device)
     native_build.build()
     stream = torch.cuda.current_stream(device)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     inst = qubo_uniform_edges(SEED, N_NODES, N_EDGES)
     lib = praq.Library()
@@ -394,9 +382,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     mixed.close()
     fp64.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
