@@ -58,6 +58,11 @@ constexpr int kXClassRows[kXClasses] = {127, 255, 511, pria::kMaxPeriods + 1};  
 enum Count { kNode = 0, kEdge, kQLow, kUp, kJLow, kQCheck, kJCheck, kY, kX0 };
 constexpr int kYZ0 = kX0 + kXClasses;
 constexpr int kMaxGroups = 17;   // y/z cluster sizes 1..16
+// JRPs of at least this many packed entries run their step kernels as their
+// own launches (the solo solver's grids, each instance a branch of the graph);
+// the smaller ones share the table-driven persistent kernels.
+constexpr long long kBigJrp = 1LL << 20;
+constexpr size_t kBigStream0 = 32;   // auxiliary streams of the big JRPs start here
 constexpr int kCounts = kYZ0 + kMaxGroups;
 
 // --- batched kernels: persistent grids over the work tables ---------------
@@ -314,6 +319,7 @@ struct Engine final : EngineBase {
     bool groups[kMaxGroups] = {};
     bool xclasses[kXClasses] = {};
     bool graph_q = false, graph_j = false;   // the captured block has QUBO / JRP work
+    std::vector<int> jbig;                    // running big JRPs in the captured block
     static constexpr int tw = pria::kXTile;
     bool dirty = true;          // the graph must be captured again
     cudaGraph_t graph = nullptr;
@@ -473,13 +479,16 @@ struct Engine final : EngineBase {
         }
         // JRP: x tiles sorted by rows (cost), y/z tasks by block size
         std::vector<std::pair<long long, int2>> xt[kXClasses], yzt[kMaxGroups], upt, yt;
+        std::vector<int> big_now;
         for (int k = 0; k < int(j.size()); ++k) {
             auto& ji = j[k];
             if (!ji.s || !ji.started || ji.done) continue;
             live.host[q.size() + k] = 1;
             auto& s = *ji.s;
             const int n = s.n, tp = s.tp, ntc = s.d.ntc;
-            for (int t = 0; t < n * ntc; ++t) {
+            const bool big = s.nd >= kBigJrp;
+            if (big) big_now.push_back(k);
+            for (int t = 0; !big && t < n * ntc; ++t) {
                 const int ctile = ntc - 1 - t / n;
                 const int rows = std::min(tp, (ctile + 1) * s.tw);
                 int cls = 0;
@@ -487,14 +496,16 @@ struct Engine final : EngineBase {
                 xt[cls].emplace_back((long long)rows, make_int2(k, t));
             }
             const int c = s.d.csize;
-            gr[c] = true;
-            ys[c] = std::max(ys[c], s.yz_smem);
+            if (!big) {
+                gr[c] = true;
+                ys[c] = std::max(ys[c], s.yz_smem);
+            }
             for (int sb = 0; sb < tp; ++sb) {
-                yzt[c].emplace_back((long long)n * (tp - sb), make_int2(k, sb));
+                if (!big) yzt[c].emplace_back((long long)n * (tp - sb), make_int2(k, sb));
                 upt.emplace_back((long long)n * (tp - sb), make_int2(k, sb));
             }
             for (int t = 0; t < s.nblo; ++t) t_jlow.host.push_back(make_int2(k, t));
-            for (int t = 0; t < s.nby; ++t) {
+            for (int t = 0; !big && t < s.nby; ++t) {
                 const long long row = (long long)t * (pria::kYThreads / 32);
                 yt.emplace_back((long long)(tp - int(row / n)), make_int2(k, t));   // row length
             }
@@ -505,6 +516,10 @@ struct Engine final : EngineBase {
             for (auto& e : v) out.host.push_back(e.second);
         };
         const bool run_q = !l_qcheck.host.empty(), run_j = !l_jcheck.host.empty();
+        if (big_now != jbig) {
+            jbig = big_now;
+            dirty = true;
+        }
         if (run_q != graph_q || run_j != graph_j) {
             graph_q = run_q;
             graph_j = run_j;
@@ -738,6 +753,36 @@ struct Engine final : EngineBase {
                 for (size_t a = 1; a < k; ++a) RB_CUDA_TRY(order_after(aux[a], stream));
                 return cudaSuccess;
             };
+            // every big JRP runs its own step chain (the solo kernels) on its own
+            // branch, beside the table-driven chain of the small ones
+            auto big_fork = [&]() -> cudaError_t {
+                for (size_t b = 0; b < jbig.size(); ++b) {
+                    cudaStream_t st;
+                    RB_CUDA_TRY(aux_stream(kBigStream0 + b, &st));
+                    RB_CUDA_TRY(order_after(stream, st));
+                }
+                return cudaSuccess;
+            };
+            auto big_join = [&]() -> cudaError_t {
+                for (size_t b = 0; b < jbig.size(); ++b) RB_CUDA_TRY(order_after(aux[kBigStream0 + b], stream));
+                return cudaSuccess;
+            };
+            RB_CUDA_TRY(big_fork());
+            for (size_t b = 0; b < jbig.size(); ++b) {
+                auto& sv = *j[jbig[b]].s;
+                cudaStream_t st = aux[kBigStream0 + b];
+                for (int s = 0; s < op_steps; ++s) {
+                    auto& dv = sv.d;
+                    if (s + 1 < op_steps) {
+                        RB_CUDA_TRY((sv.template launch_x<true, false>(dv.xh, dv.yh, dv.zh, s, 0, st)));
+                        RB_CUDA_TRY((sv.template launch_yz<true, false>(dv.yh, dv.zh, s, 0, st)));
+                    } else {
+                        RB_CUDA_TRY((sv.template launch_x<true, true>(dv.xh, dv.yh, dv.zh, s, 0, st)));
+                        RB_CUDA_TRY((sv.template launch_yz<true, true>(dv.yh, dv.zh, s, 0, st)));
+                    }
+                    nodes += 3;
+                }
+            }
             for (int s = 0; s < op_steps; ++s) {
                 const bool last = s + 1 == op_steps;
                 RB_CUDA_TRY(x_stage([&](int c, cudaStream_t st) {
@@ -749,14 +794,26 @@ struct Engine final : EngineBase {
                         return last ? launch_yz<true, true>(c, s, 0, st) : launch_yz<true, false>(c, s, 0, st);
                     }));
             }
+            RB_CUDA_TRY(big_join());
             bj_upper<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_up.buf.ptr, counts.ptr + kUp);
             bj_lower<Real><<<sms * 8, pria::kAuxThreads, 0, stream>>>(jdevs.buf.ptr, t_jlow.buf.ptr, counts.ptr + kJLow);
             bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
                                                                      counts.ptr + kJCheck, 1);
             nodes += 3;
+            // the gated restart step: big ones on their branches, small ones by tables
+            RB_CUDA_TRY(big_fork());
+            for (size_t b = 0; b < jbig.size(); ++b) {
+                auto& sv = *j[jbig[b]].s;
+                auto& dv = sv.d;
+                cudaStream_t st = aux[kBigStream0 + b];
+                RB_CUDA_TRY((sv.template launch_x<false, true>(dv.x2s, dv.y2s, dv.z2s, 0, 1, st)));
+                RB_CUDA_TRY((sv.template launch_yz<false, true>(dv.y2s, dv.z2s, 0, 1, st)));
+                nodes += 3;
+            }
             RB_CUDA_TRY(x_stage([&](int c, cudaStream_t st) { return launch_x<false, true>(c, 0, 1, st); }));
             RB_CUDA_TRY(yz_stage([&](cudaStream_t st) { return launch_y<false, true>(0, 1, st); },
                                  [&](int c, cudaStream_t st) { return launch_yz<false, true>(c, 0, 1, st); }));
+            RB_CUDA_TRY(big_join());
             bj_check<Real><<<sms * 4, pria::kCheckBlock, 0, stream>>>(jdevs.buf.ptr, jmeta.buf.ptr, l_jcheck.buf.ptr,
                                                                      counts.ptr + kJCheck, 2);
             nodes += 1;
@@ -781,8 +838,9 @@ struct Engine final : EngineBase {
         int ex = 0, eg = 0;
         for (bool b : xclasses) ex += b;
         for (bool b : groups) eg += b;
-        const size_t wide = size_t(std::max(ex, eg)) + 1;
-        const size_t events_needed = 2 + size_t(op_steps + 1) * 2 * size_t(std::max(0, ex - 1) + eg);
+        const size_t wide = std::max(size_t(std::max(ex, eg)) + 1, kBigStream0 + jbig.size());
+        const size_t events_needed =
+            2 + size_t(op_steps + 1) * 2 * size_t(std::max(0, ex - 1) + eg) + 4 * jbig.size();
         cudaStream_t tmp;
         if (aux_stream(wide, &tmp)) return -int(cudaErrorUnknown);
         while (fj.size() < events_needed) {

@@ -1234,22 +1234,24 @@ struct Solver final : SolverBase {
     bool vanilla_phase() const { return !p.use_halpern || p.warm_steps > 0; }
 
     template <bool R, bool C>
-    cudaError_t launch_x(const Real* xs, const Real* ys, const Real* zs, int step, int gate) {
-        x_kernel<Real, kXTile, R, C><<<n * d.ntc, kXThreads, x_smem, stream>>>(d, xs, ys, zs, step, gate);
+    cudaError_t launch_x(const Real* xs, const Real* ys, const Real* zs, int step, int gate,
+                         cudaStream_t on = nullptr) {
+        x_kernel<Real, kXTile, R, C><<<n * d.ntc, kXThreads, x_smem, on ? on : stream>>>(d, xs, ys, zs, step, gate);
         return cudaGetLastError();
     }
 
     template <bool R, bool C>
     // the y half-step (one warp per row) and then the z half-step (a cluster
     // per period block); two launches
-    cudaError_t launch_yz(const Real* ys, const Real* zs, int step, int gate) {
-        y_kernel<Real, R, C><<<nby, kYThreads, size_t(kYThreads / 32) * tp * sizeof(Real), stream>>>(d, ys, step, gate);
+    cudaError_t launch_yz(const Real* ys, const Real* zs, int step, int gate, cudaStream_t on = nullptr) {
+        cudaStream_t st = on ? on : stream;
+        y_kernel<Real, R, C><<<nby, kYThreads, size_t(kYThreads / 32) * tp * sizeof(Real), st>>>(d, ys, step, gate);
         RB_CUDA_TRY(cudaGetLastError());
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(unsigned(tp * d.csize));
         cfg.blockDim = dim3(kZThreads);
         cfg.dynamicSmemBytes = yz_smem;
-        cfg.stream = stream;
+        cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = unsigned(d.csize);
