@@ -61,20 +61,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n: int, m: int, real: int, index: int = 4, op_steps: int = 16) -> dict:
+def algorithmic_bytes(n: int, m: int, real: int, index: int = 4) -> dict:
     """Per-launch algorithmic bytes of the two step kernels.  The per-iteration
     total is the PRAQ figure n (6R + I) + m (11R + 4I): the node kernel reads
     x (predicted), x0, diag, deg and the CSR pointer and writes x, r
     (n (6R + I)) and reads the CSR index and one gathered dual per half-edge
     (m (2I + 2R)); the edge kernel reads both ends, the weight, the predicted
     dual pair, the anchor pair and r at both ends and writes the dual pair
-    (m (2I + 9R)).  The persistent block kernel runs op_steps iterations and
-    the lower-bound pass (n (2R + I) + 2 m R) per launch."""
+    (m (2I + 9R))."""
     node = n * (6 * real + index) + m * (2 * index + 2 * real)
     edge = m * (2 * index + 9 * real)
-    lower = n * (2 * real + index) + 2 * m * real
     return {"node": node, "edge": edge, "node_check": node, "edge_check": edge,
-            "iteration": node + edge, "block": op_steps * (node + edge) + lower}
+            "iteration": node + edge}
 
 
 class ClockSampler:

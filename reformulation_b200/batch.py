@@ -205,7 +205,7 @@ class EscalatingBatch:
     object's own.
     """
 
-    def __init__(self, stream: int | None = None, stall_iterations: int = 1024,
+    def __init__(self, stream: int | None = None, stall_iterations: int = 384,
                  fp64_parameters=None):
         self.b32 = Batch("mixed", stream)
         self.b64: Batch | None = None

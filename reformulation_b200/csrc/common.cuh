@@ -108,35 +108,6 @@ __device__ __forceinline__ T clampv(T v, T lo, T hi) {
     return v < lo ? lo : (v > hi ? hi : v);
 }
 
-// A device allocation on a stream (cudaMallocAsync), released on the same
-// stream.  The caller owns the stream and synchronises before it goes away.
-template <class T>
-struct DevBuf {
-    T* ptr = nullptr;
-    size_t count = 0;
-    cudaStream_t stream = nullptr;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (ptr) cudaFreeAsync(ptr, stream);
-        ptr = nullptr;
-        count = 0;
-    }
-    cudaError_t alloc(size_t n, cudaStream_t s) {
-        release();
-        stream = s;
-        count = n;
-        return cudaMallocAsync(reinterpret_cast<void**>(&ptr), sizeof(T) * (n ? n : 1), s);
-    }
-    cudaError_t upload(const T* host, size_t n, cudaStream_t s) {
-        RB_CUDA_TRY(alloc(n, s));
-        if (n) RB_CUDA_TRY(cudaMemcpyAsync(ptr, host, sizeof(T) * n, cudaMemcpyHostToDevice, s));
-        return cudaSuccess;
-    }
-};
-
 inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
 
 }  // namespace rb200

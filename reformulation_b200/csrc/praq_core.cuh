@@ -111,10 +111,16 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
     return c->terminated || (gate && !c->restart);
 }
 
-#ifndef RB200_PRAQ_STAGE
-#define RB200_PRAQ_STAGE 512   // compile-time tunable (sweeps build with -D)
+#ifndef RB200_PRAQ_STAGE_BYTES
+#define RB200_PRAQ_STAGE_BYTES 2048   // per warp and pass; compile-time tunable (sweeps build with -D)
 #endif
-constexpr int kStage = RB200_PRAQ_STAGE;   // half-edge values a warp stages per pass
+#ifndef RB200_PRAQ_STAGE_UNROLL
+#define RB200_PRAQ_STAGE_UNROLL 4
+#endif
+constexpr int kStageUnroll = RB200_PRAQ_STAGE_UNROLL;
+// half-edge values a warp stages per pass
+template <class Real>
+constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 
 // The sums of v over the runs [ptr[i], ptr[i+1]) of the 32 consecutive nodes
 // i = base + lane of a warp, one node per lane.  The runs of consecutive nodes
@@ -134,10 +140,11 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
         a = ptr[i];
         b = ptr[i + 1];
     }
+    constexpr int kStage = stage_len<Real>();
     Acc s = Acc(0);
     for (int c0 = lo_all; c0 < hi_all; c0 += kStage) {
         const int c1 = min(hi_all, c0 + kStage);
-#pragma unroll 4
+#pragma unroll kStageUnroll
         for (int k = c0 + lane; k < c1; k += 32) stage[k - c0] = v[k];
         __syncwarp();
         const int lo = max(a, c0), hi = min(b, c1);
@@ -168,7 +175,7 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
     __shared__ double scratch[kNodeSums * 32];
-    __shared__ Real stage[kBlock / 32][kStage];
+    __shared__ Real stage[kBlock / 32][stage_len<Real>()];
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
@@ -315,7 +322,7 @@ template <class Real>
 __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     if (d.ctl->terminated) return;
     __shared__ double scratch[32];
-    __shared__ Real stage[kBlock / 32][kStage];
+    __shared__ Real stage[kBlock / 32][stage_len<Real>()];
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;

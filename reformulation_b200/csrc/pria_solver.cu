@@ -1,6 +1,7 @@
 // pria_solver.cu -- the C ABI of the PRIA solver (include/pria.h); the
 // solver itself (kernels, device layout, host driver) is pria_core.cuh.
 #include "pria_core.cuh"
+#include "../../include/reform.h"
 
 using namespace rb200;
 
@@ -32,10 +33,57 @@ static int solve_one(int64_t n, int64_t t, const T* k, T k0, const T* h, const p
     }
 }
 
+struct BatchGuard {
+    reform_batch* b;
+    ~BatchGuard() { reform_batch_destroy(b); }
+};
+
+// The reference's batch call (jrp/pria-cuda/src/pria.cu:15-44 fans independent
+// solves out over host threads and streams) as one batched engine
+// (include/reform.h): every instance in the same graph replays, each result
+// bitwise its solo solve.  The engine runs the restarted Halpern method; plain
+// PDHG or a vanilla warm phase falls back to solo solves one after another.
+template <class T>
+static int solve_batch_engine(int64_t count, int64_t n, int64_t t, const T* k, const T* k0, const T* h,
+                              const pria_params* params, T* x, T* y, T* z, pria_result_info* infos) {
+    const int64_t full = n * t * t;
+    reform_batch* b = nullptr;
+    int st = reform_batch_create(sizeof(T) == 4 ? 1 : 0, nullptr, &b);
+    if (st) return st < 0 ? -st : st;
+    const BatchGuard guard{b};
+    std::vector<int> slot;
+    for (int64_t i = 0; i < count; ++i) {
+        const std::vector<double> costs(k + i * n, k + (i + 1) * n);
+        const std::vector<double> holding(h + i * full, h + (i + 1) * full);
+        const int id = reform_batch_add_jrp(b, n, t, costs.data(), double(k0[i]), holding.data(), params);
+        if (id < 0) return -id;
+        slot.push_back(id);
+    }
+    if ((st = reform_batch_start(b)) || (st = reform_batch_run(b, -1))) return st < 0 ? -st : st;
+    std::vector<double> xd, yd, zd;
+    if (x) xd.resize(size_t(full));
+    if (y) yd.resize(size_t(full));
+    if (z) zd.resize(size_t(full));
+    for (int64_t i = 0; i < count; ++i) {
+        st = reform_batch_result_jrp(b, slot[size_t(i)], x ? xd.data() : nullptr, y ? yd.data() : nullptr,
+                                     z ? zd.data() : nullptr, infos ? infos + i : nullptr);
+        if (st) return st < 0 ? -st : st;
+        for (int64_t a = 0; a < full; ++a) {
+            if (x) x[i * full + a] = T(xd[size_t(a)]);
+            if (y) y[i * full + a] = T(yd[size_t(a)]);
+            if (z) z[i * full + a] = T(zd[size_t(a)]);
+        }
+    }
+    return 0;
+}
+
 template <class T>
 static int solve_batch(int64_t count, int64_t n, int64_t t, const T* k, const T* k0, const T* h,
                        const pria_params* params, T* x, T* y, T* z, pria_result_info* infos) {
-    if (count <= 0 || !k || !k0 || !h) return int(cudaErrorInvalidValue);
+    if (count <= 0 || !k || !k0 || !h || !params) return int(cudaErrorInvalidValue);
+    if (n < 1 || t < 1) return int(cudaErrorInvalidValue);
+    if (params->use_halpern && params->warm_steps <= 0)
+        return solve_batch_engine<T>(count, n, t, k, k0, h, params, x, y, z, infos);
     const int64_t full = n * t * t;
     int err = 0;
     for (int64_t b = 0; b < count; ++b) {
