@@ -349,6 +349,18 @@ def run_ours(args):
             "wall_s_timed_region": wall,
         }
 
+    # the objective against the exact roof dual (max-flow) and the FP64 run
+    if rank == 0 and not args.skip_cpu:
+        import oracle
+        flow = oracle.roof_dual_maxflow(inst)
+        line["objective_check"] = {
+            "maxflow_roof_dual": flow,
+            "mixed_upper_rel_err": abs(res.upper - flow) / (1.0 + abs(flow)),
+            "fp64_upper_rel_err": abs(res64.upper - flow) / (1.0 + abs(flow)),
+            "mixed_vs_fp64_upper_rel": abs(res.upper - res64.upper) / (1.0 + abs(res64.upper)),
+            "brackets_contain_optimum": bool(res.lower <= flow + 1e-9 * abs(flow) <= res.upper + 2e-9 * abs(flow)
+                                             and res64.lower <= flow + 1e-9 * abs(flow) <= res64.upper + 2e-9 * abs(flow))}
+
     # CPU baseline and the reference's own praq-cuda, rank 0 at N=1 only
     if rank == 0 and world == 1 and not args.skip_cpu:
         threads = cpu_threads()
@@ -432,6 +444,8 @@ def run_pria(args):
             "value": out["mixed"]["solves_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "mixed": out["mixed"], "plain_fp64": out["fp64"],
             "mixed_vs_fp64": out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"],
+            "mixed_objective_rel_err_vs_fp64": abs(out["mixed"]["upper"] - out["fp64"]["upper"])
+                                               / (1.0 + abs(out["fp64"]["upper"])),
             "peak_hbm_gbs": peaks()[0], "data": "synthetic"}
     print(json.dumps(line), flush=True)
     return 0
