@@ -112,13 +112,17 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
 }
 
 #ifndef RB200_PRAQ_STAGE_BYTES
-#define RB200_PRAQ_STAGE_BYTES 2048   // per warp and pass; compile-time tunable (sweeps build with -D)
+#define RB200_PRAQ_STAGE_BYTES 2048   // per warp, run and pass; compile-time tunable (sweeps build with -D)
 #endif
 #ifndef RB200_PRAQ_STAGE_UNROLL
 #define RB200_PRAQ_STAGE_UNROLL 4
 #endif
+#ifndef RB200_PRAQ_GATHER
+#define RB200_PRAQ_GATHER 2   // node gather: 0 one run after the other, 1 both at once, 2 by grid size
+#endif
 constexpr int kStageUnroll = RB200_PRAQ_STAGE_UNROLL;
-// half-edge values a warp stages per pass
+constexpr int kGather = RB200_PRAQ_GATHER;
+// half-edge values a warp stages per run and pass
 template <class Real>
 constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 
@@ -127,7 +131,8 @@ constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 // are adjacent, so the warp copies the whole range [ptr[base], ptr[base+32])
 // through shared memory in coalesced passes of kStage values, and each lane
 // adds its own run's part of every pass in order.  All lanes of the warp must
-// call it (with the same base).
+// call it (with the same base).  Few registers: the form for grids of many
+// waves, where the issue rate, not the latency of one warp, bounds the kernel.
 template <class Real, class Acc>
 __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v, int n,
                                          long long base, int lane, Real* __restrict__ stage) {
@@ -154,28 +159,100 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
     return s;
 }
 
-// S^T y at node base + lane: the node's run of `ys` (first-end order) plus its
-// run of `yc` (second-end order).
+// The sums, for the 32 consecutive nodes i = base + lane of a warp (one node
+// per lane), of two runs at once: run a = va[pa[i] .. pa[i+1]) and run b =
+// vb[pb[i] .. pb[i+1]).  The warp copies the ranges va[pa[base] .. pa[base+32])
+// and vb[pb[base] .. pb[base+32]) through shared memory in coalesced passes of
+// kStage values each, and every lane adds its own runs' parts of each pass in
+// order.  A pass's loads, of both ranges, are predicated loads into registers
+// with no loop around them, so all of them are in flight together: one memory
+// round trip per pass (a warp-uniform exit skips the slots past both ranges).
+// The sums are those of warp_runs, term for term and in the same order.
+// Twice the registers of warp_runs: the form for grids of one wave, which the
+// latency of a warp's dependent loads bounds.  All lanes of the warp must call
+// it with the same base.
 template <class Real, class Acc>
+__device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Real* __restrict__ va,
+                                           const int* __restrict__ pb, const Real* __restrict__ vb,
+                                           int n, long long base, int lane, Real* __restrict__ sa,
+                                           Real* __restrict__ sb, Acc& ra, Acc& rb) {
+    ra = Acc(0);
+    rb = Acc(0);
+    if (base >= n) return;   // uniform over the warp
+    const long long i = base + lane;
+    const long long last = base + 32 < n ? base + 32 : n;
+    const int alo = pa[base], ahi = pa[last], blo = pb[base], bhi = pb[last];
+    int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    if (i < n) {
+        a0 = pa[i];
+        a1 = pa[i + 1];
+        b0 = pb[i];
+        b1 = pb[i + 1];
+    }
+    constexpr int kStage = stage_len<Real>();
+    constexpr int kPer = kStage / 32;
+    static_assert(kStage % 32 == 0, "a pass is whole warp rows");
+    for (int ca = alo, cb = blo; ca < ahi || cb < bhi; ca += kStage, cb += kStage) {
+        const int ea = min(ahi, ca + kStage), eb = min(bhi, cb + kStage);
+        // lane-relative bases and counts, so each load is a base plus an
+        // immediate offset
+        const Real* __restrict__ ga = va + (ca + lane);
+        const Real* __restrict__ gb = vb + (cb + lane);
+        const int na = ea - ca - lane, nb = eb - cb - lane;
+        const int wide = max(ea - ca, eb - cb);   // the same on every lane
+        Real ta[kPer], tb[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            if (32 * q >= wide) break;
+            if (32 * q < na) ta[q] = ga[32 * q];
+            if (32 * q < nb) tb[q] = gb[32 * q];
+        }
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            if (32 * q >= wide) break;
+            if (32 * q < na) sa[lane + 32 * q] = ta[q];
+            if (32 * q < nb) sb[lane + 32 * q] = tb[q];
+        }
+        __syncwarp();
+        for (int k = max(a0, ca), e = min(a1, ea); k < e; ++k) ra += Acc(sa[k - ca]);
+        for (int k = max(b0, cb), e = min(b1, eb); k < e; ++k) rb += Acc(sb[k - cb]);
+        __syncwarp();
+    }
+}
+
+// S^T y at node base + lane: the node's run of `ys` (first-end order) plus its
+// run of `yc` (second-end order).  `stage` holds stage_runs<Wide> * stage_len
+// values; both forms give the same sum.
+template <bool Wide>
+constexpr int stage_runs() { return Wide ? 2 : 1; }
+
+template <class Real, class Acc, bool Wide>
 __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __restrict__ ys,
                                           const Real* __restrict__ yc, long long base, int lane,
                                           Real* __restrict__ stage) {
-    const Acc s0 = warp_runs<Real, Acc>(d.row_ptr, ys, d.n, base, lane, stage);
-    const Acc s1 = warp_runs<Real, Acc>(d.col_ptr, yc, d.n, base, lane, stage);
-    return s0 + s1;
+    if constexpr (Wide) {
+        Acc s0, s1;
+        warp_runs2<Real, Acc>(d.row_ptr, ys, d.col_ptr, yc, d.n, base, lane, stage,
+                              stage + stage_len<Real>(), s0, s1);
+        return s0 + s1;
+    } else {
+        const Acc s0 = warp_runs<Real, Acc>(d.row_ptr, ys, d.n, base, lane, stage);
+        const Acc s1 = warp_runs<Real, Acc>(d.col_ptr, yc, d.n, base, lane, stage);
+        return s0 + s1;
+    }
 }
 
 // Primal half of one PDHG step, with the Halpern combination of x folded in
 // (solver.py:259-267 and 276-292).  Reflect: x1 = lw (2 x2 - x1) + rw x0 with
 // k = restart_iter + step + 1; vanilla: x1 = x2 and the anchor becomes x1.
 // Check: the node sums of this step go to pnode.
-template <class Real, bool Reflect, bool Check>
+template <class Real, bool Reflect, bool Check, bool Wide = false>
 __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
             int bounds_at_1, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
     __shared__ double scratch[kNodeSums * 32];
-    __shared__ Real stage[kBlock / 32][stage_len<Real>()];
+    __shared__ Real stage[kBlock / 32][stage_runs<Wide>() * stage_len<Real>()];
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
@@ -191,7 +268,7 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
             x0o = d.x0[i];
         }
     }
-    const Real s = scatter_at<Real, Real>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const Real s = scatter_at<Real, Real, Wide>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[kNodeSums] = {0.0, 0.0, 0.0};
     if (owner) {
         Real x1v;
@@ -224,13 +301,13 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
     }
 }
 
-template <class Real, bool Reflect, bool Check>
+template <class Real, bool Reflect, bool Check, bool Wide = false>
 __global__ void __launch_bounds__(kBlock)
 node_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
             int bounds_at_1, int gate) {
     pdl_wait();
     pdl_launch_dependents();
-    node_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ys, yc, step, bounds_at_1, gate);
+    node_kernel_tile<Real, Reflect, Check, Wide>(d, blockIdx.x, ys, yc, step, bounds_at_1, gate);
 }
 
 // Dual half of one PDHG step (solver.py:269-273, projection.py:16-42) in the
@@ -318,15 +395,15 @@ edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) 
 
 // The node part of the lower bound, sum_i min(d_i - (S^T y)_i, 0), at the
 // dual (ys, yc) (solver.py:333-337), in FP64.
-template <class Real>
+template <class Real, bool Wide = false>
 __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     if (d.ctl->terminated) return;
     __shared__ double scratch[32];
-    __shared__ Real stage[kBlock / 32][stage_len<Real>()];
+    __shared__ Real stage[kBlock / 32][stage_runs<Wide>() * stage_len<Real>()];
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
-    const double s = scatter_at<Real, double>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const double s = scatter_at<Real, double, Wide>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[1] = {0.0};
     if (i < d.n) {
         const double rc = double(d.diag[i]) - s;
@@ -336,12 +413,12 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
     if (threadIdx.x == 0) d.plower[tile] = acc[0];
 }
 
-template <class Real>
+template <class Real, bool Wide = false>
 __global__ void __launch_bounds__(kBlock)
 lower_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     pdl_wait();
     pdl_launch_dependents();
-    lower_kernel_tile<Real>(d, blockIdx.x, ys, yc);
+    lower_kernel_tile<Real, Wide>(d, blockIdx.x, ys, yc);
 }
 
 __device__ __forceinline__ double canonical(const double* node, const double* edge, double omega) {
@@ -634,6 +711,7 @@ struct Solver final : SolverBase {
     Control* mirror = nullptr;   // pinned host copy of the control block
     Dev<Real> d{};
     int nb_node = 1, nb_edge = 1;
+    bool wide = false;   // node gather of both runs at once (warp_runs2)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
@@ -674,6 +752,16 @@ struct Solver final : SolverBase {
         if (st) return st;
         nb_node = ceil_div(n, kBlock);   // one node per thread
         nb_edge = std::max(1, ceil_div(m, kBlock * kEdgesPerThread));
+        // The wide gather halves a warp's chain of dependent loads but takes
+        // twice the registers: it wins while the node grid is one wave of it.
+        {
+            int dev = 0, sms = 0, per_sm = 0;
+            if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, node_kernel<Real, true, false, true>,
+                                                              kBlock, 0))
+                return PRAQ_ERROR_CUDA;
+            wide = kGather == 1 || (kGather == 2 && nb_node <= sms * per_sm);
+        }
         for (auto* b : {&x1, &x2, &x0, &r})
             if (b->alloc(n, stream)) return PRAQ_ERROR_CUDA;
         for (auto* b : {&pred, &predc, &u0, &u2s, &u2c})
@@ -803,21 +891,24 @@ struct Solver final : SolverBase {
     // One op_steps block: op_steps reflected steps (the last with the check
     // sums), the lower-bound pass, the check, then the restart step (gated on
     // the device flag), its error, and a copy of the control block to the host.
-    cudaError_t enqueue_block() {
+    cudaError_t enqueue_block() { return wide ? enqueue_steps<true>() : enqueue_steps<false>(); }
+
+    template <bool W>
+    cudaError_t enqueue_steps() {
         const int op = int(p.op_steps);
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
-                RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
+                RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false, W>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
                 if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, false>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             } else {
-                RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
+                RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true, W>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
                 if (m) RB_TIMED(3, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, true>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             }
         }
-        RB_TIMED(4, RB_CUDA_TRY(launch_pdl(lower_kernel<Real>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c)));
+        RB_TIMED(4, RB_CUDA_TRY(launch_pdl(lower_kernel<Real, W>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c)));
         RB_TIMED(5, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 1)));
-        RB_TIMED(6, RB_CUDA_TRY(launch_pdl(node_kernel<Real, false, true>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c, 0, 0, 1)));
+        RB_TIMED(6, RB_CUDA_TRY(launch_pdl(node_kernel<Real, false, true, W>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c, 0, 0, 1)));
         if (m) RB_TIMED(7, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, false, true>, nb_edge, kBlock, stream, d, (const Real*)d.u2s, 0, 0, 1)));
         RB_TIMED(8, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 2)));
