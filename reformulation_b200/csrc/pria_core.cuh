@@ -104,7 +104,10 @@ __host__ __device__ __forceinline__ long long blk(int n, int tp, int s) {
 template <class Real>
 struct Dev {
     int n, t, tp, ntc, ntc_low, csize;
-    int zstaged;             // 1: z + r of a block sits in its cluster's shared memory;
+    int zpair;               // 1: the solver's z launch takes period blocks in pairs (s, Tp - 1 - s)
+                             //    (z_task_pair); 0: one block per cluster (z_task, which the
+                             //    batched engine always uses; the slice fits either way)
+    int zstaged;             // 1: z + r of a task sits in its cluster's shared memory;
                              // 0: too large for that, every Michelot round recomputes
                              //    it from global memory (L2-resident)
     long long nd;
@@ -412,6 +415,66 @@ y_kernel(Dev<Real> d, const Real* ysrc, int step, int gate) {
     y_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ysrc, step, gate, reinterpret_cast<Real*>(smem_raw), d.tp);
 }
 
+// michelot() advanced one evaluation at a time, so that several problems can
+// share each (cluster-wide) evaluation: init, then while !done() evaluate the
+// sums (S, C) over {v > th} (all v when th is -inf) and feed() them.  The
+// steps and decisions are michelot()'s, one for one; th is the result once
+// done().
+struct MichelotSteps {
+    double target, th, S;
+    int C, len, round, stage;   // stage 0: warm pending, 1: all-active pending, 2: round pending, 3: done
+    bool monotone;
+    __device__ __forceinline__ void init(double tgt, double warm, int n_) {
+        target = tgt;
+        len = n_;
+        round = 0;
+        S = 0.0;
+        C = 0;
+        monotone = true;
+        if (!(tgt > 0.0)) {
+            th = INFINITY;
+            stage = 3;
+        } else if (isfinite(warm)) {
+            th = warm;
+            stage = 0;
+        } else {
+            th = -INFINITY;
+            stage = 1;
+        }
+    }
+    __device__ __forceinline__ bool done() const { return stage == 3; }
+    __device__ __forceinline__ void feed(double S2, int C2) {
+        if (stage == 0) {
+            S = S2;
+            C = C2;
+            monotone = false;
+            if (C == 0) {
+                th = -INFINITY;
+                stage = 1;
+            } else {
+                th = (S - target) / double(C);
+                stage = 2;
+            }
+        } else if (stage == 1) {
+            S = S2;
+            C = C2;
+            monotone = true;
+            th = (S - target) / double(C);
+            stage = 2;
+        } else if (stage == 2) {
+            if (C2 == C || C2 == 0 || (monotone && C2 > C)) {
+                stage = 3;
+                return;
+            }
+            monotone = true;
+            S = S2;
+            C = C2;
+            th = (S2 - target) / double(C2);
+            if (++round > len) stage = 3;
+        }
+    }
+};
+
 // z half-step (solver.py:423) for period block s, one cluster of `csize` CTAs
 // per block; CTA `rank` owns rows [r0, r1) of the block, a contiguous slice.
 // z + r of the slice goes to shared memory, the threshold of the whole block
@@ -537,10 +600,174 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
     }
 }
 
+// z half-step (solver.py:423) for the pair of period blocks s = pair and
+// s = Tp - 1 - pair (N (Tp - s) entries each, N (Tp + 1) together, so every
+// pair is the same work), one cluster of `csize` CTAs per pair; CTA `rank`
+// owns rows [r0, r1) of both blocks, a contiguous slice of each.  z + r of
+// the slices goes to shared memory; each block's threshold comes from its own
+// Michelot rounds, the two blocks' rounds taken together, so one cluster
+// barrier passes both blocks' (sum, count) through distributed shared memory;
+// then the slices' z is written.  Every per-block sum is taken in z_task's
+// order, so the results are z_task's, bit for bit; the check partials go to
+// each block's own rows of pyz.  Half the clusters of z_task, each with twice
+// the entries per barrier: it pays when the pairs still fill the GPU and
+// the CTAs are few per SM (FP64, register-bound to one per SM).
 template <class Real, int kThreads, bool Reflect, bool Check>
+__device__ __forceinline__ void z_task_pair(const Dev<Real>& d, int pair, const Real* zsrc, int step, int gate) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
+    cg::cluster_group cluster = cg::this_cluster();
+    const int csize = d.csize;
+    const int rank = int(cluster.block_rank());
+    const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real* vz = reinterpret_cast<Real*>(smem_raw);
+    __shared__ double part[2][4];
+    __shared__ double scratch[6 * 32];
+    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
+    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    const bool vanilla = !Reflect && (gate & kGateVanilla);   // as in the y half-step
+    const bool drift = Reflect || (gate & kGateDrift);
+    const int sblk[2] = {pair, d.tp - 1 - pair};
+    int len[2], mine[2], off[2];
+    long long sbase[2];
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+        len[g] = d.tp - sblk[g];
+        mine[g] = (r1 - r0) * len[g];
+        sbase[g] = blk(d.n, d.tp, sblk[g]) + (long long)r0 * len[g];
+    }
+    off[0] = 0;
+    off[1] = mine[0];
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // per block: |dz|^2, <dx, dz>, drift
+
+    const bool staged = d.zstaged != 0;
+    // v(g, q) = z + r of element q of block g's slice, in the same arithmetic either way
+    auto vval = [&](int g, int q) -> Real {
+        return staged ? vz[off[g] + q] : Real(zsrc[sbase[g] + q] + d.r[sbase[g] + q]);
+    };
+
+    // phase A: z + r of the slices into shared memory, kZUnroll loads in flight
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+        for (int qb = threadIdx.x; staged && qb < mine[g]; qb += kThreads * kZUnroll) {
+            Real zv[kZUnroll], rv[kZUnroll];
+#pragma unroll
+            for (int u = 0; u < kZUnroll; ++u) {
+                const int q = qb + u * kThreads;
+                if (q < mine[g]) {
+                    zv[u] = zsrc[sbase[g] + q];
+                    rv[u] = d.r[sbase[g] + q];
+                    if (drift && (q & 7) == 0) prefetch_l2(d.z0 + sbase[g] + q);
+                    if (Check && (q & 7) == 0) prefetch_l2(d.dxs + sbase[g] + q);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kZUnroll; ++u) {
+                const int q = qb + u * kThreads;
+                if (q < mine[g]) vz[off[g] + q] = zv[u] + rv[u];
+            }
+        }
+    }
+    __syncthreads();
+
+    // phase B: each block's z threshold across the cluster.  Each CTA's
+    // (sum, count) per block over its slice goes to part[parity]; after one
+    // cluster barrier every CTA adds all ranks' partials in rank order, so
+    // every CTA takes the same decisions.  The two parities let a round write
+    // its partials while no CTA can still be reading that buffer.
+    MichelotSteps ms[2];
+#pragma unroll
+    for (int g = 0; g < 2; ++g) ms[g].init(double(d.k0), d.thz[sblk[g]], d.n * len[g]);
+    int parity = 0;
+    while (!ms[0].done() || !ms[1].done()) {
+        double b[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+            if (ms[g].done()) continue;
+            const double th = ms[g].th;
+            for (int q = threadIdx.x; q < mine[g]; q += kThreads) {
+                const double x = double(vval(g, q));
+                if (th == -INFINITY || x > th) {
+                    b[2 * g] += x;
+                    b[2 * g + 1] += 1.0;
+                }
+            }
+        }
+        block_sums<4>(b, scratch, b);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) part[parity][k] = b[k];
+        }
+        cluster.sync();
+        double tot[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int rk = 0; rk < csize; ++rk) {
+            const double* pp = cluster.map_shared_rank(&part[parity][0], rk);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) tot[k] += pp[k];
+        }
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+            if (!ms[g].done()) ms[g].feed(tot[2 * g], int(tot[2 * g + 1]));
+        parity ^= 1;
+    }
+    cluster.sync();   // no CTA leaves while another may still read its partials
+    if (rank == 0 && threadIdx.x == 0) {
+        d.thz[sblk[0]] = ms[0].th;
+        d.thz[sblk[1]] = ms[1].th;
+    }
+
+    // phase C: z
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+        const double thz = ms[g].th;
+        for (int qb = threadIdx.x; qb < mine[g]; qb += kThreads * kZUnroll) {
+            Real z1v[kZUnroll], zav[kZUnroll], dxv[kZUnroll];
+#pragma unroll
+            for (int u = 0; u < kZUnroll; ++u) {
+                const int q = qb + u * kThreads;
+                if (q < mine[g]) {
+                    z1v[u] = zsrc[sbase[g] + q];
+                    zav[u] = drift ? d.z0[sbase[g] + q] : z1v[u];
+                    if (Check) dxv[u] = d.dxs[sbase[g] + q];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kZUnroll; ++u) {
+                const int q = qb + u * kThreads;
+                if (q >= mine[g]) continue;
+                const long long e = sbase[g] + q;
+                const Real z2 = Real(fmax(double(vval(g, q)) - thz, 0.0));
+                const Real z1 = z1v[u], za = Reflect ? zav[u] : z1;
+                d.zh[e] = vanilla ? z2 : lwn * (Real(2) * z2 - z1) + rwn * za;
+                if (!Reflect && !vanilla) d.z0[e] = z1;
+                if (Check) {
+                    if (Reflect) d.z2s[e] = z2;
+                    const double dz = double(z1) - double(z2), dr = double(z1) - double(zav[u]);
+                    acc[3 * g] += dz * dz;
+                    acc[3 * g + 1] += double(dxv[u]) * dz;
+                    acc[3 * g + 2] += dr * dr;
+                }
+            }
+        }
+    }
+    if (Check) {
+        block_sums<6>(acc, scratch, acc);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int g = 0; g < 2; ++g)
+                for (int k = 0; k < 3; ++k) d.pyz[(size_t(sblk[g]) * csize + rank) * 3 + k] = acc[3 * g + k];
+        }
+    }
+}
+
+template <class Real, int kThreads, bool Reflect, bool Check, bool Pair>
 __global__ void __launch_bounds__(kThreads)
 z_kernel(Dev<Real> d, const Real* zsrc, int step, int gate) {
-    z_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
+    if constexpr (Pair)
+        z_task_pair<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
+    else
+        z_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
 }
 
 // The primal bound terms at x for period block s (solver.py:347-365):
@@ -1031,6 +1258,8 @@ struct Solver final : SolverBase {
     static constexpr size_t y_smem_limit() { return size_t(kYThreads / 32) * kMaxPeriods * sizeof(Real); }
     // x tiles: kXTile columns of a padded row of at most kMaxPeriods (+1)
     // FP64 values
+    // z tasks of the z half-step (pairs of period blocks, or blocks)
+    int z_tasks() const { return d.zpair ? tp / 2 : tp; }
     static constexpr size_t x_smem_limit() {
         return size_t(kXTile) * size_t(kMaxPeriods + 1) * sizeof(double);
     }
@@ -1143,11 +1372,29 @@ struct Solver final : SolverBase {
         nbx = n * ntc;
         nblo = n * ntc_low;
         x_smem = size_t(tw) * size_t(tp | 1) * sizeof(double);
-        int csize = 1;
-        while (csize < kMaxCluster && (size_t((n + csize - 1) / csize) * tp * sizeof(Real)) > size_t(kSliceBytes))
-            ++csize;
-        if (csize > n) csize = n;
-        yz_smem = size_t((n + csize - 1) / csize) * tp * sizeof(Real);
+        // z: a CTA of a cluster holds its rows of one period block (Tp - s
+        // entries per row; z_task), or of a pair of blocks (Tp + 1 entries
+        // per row; z_task_pair) in FP64 when the pairs still fill a wave of
+        // two CTAs per SM.  Measured per solve: FP64 pairs are 6-14 % faster
+        // at N = 10..200, T = 300..1000; in FP32 (two z CTAs per SM) and on
+        // grids under a wave, pairs are 1-7 % slower.
+        auto cluster_for = [&](int row) {
+            int c = 1;
+            while (c < kMaxCluster && size_t((n + c - 1) / c) * row * sizeof(Real) > size_t(kSliceBytes)) ++c;
+            return c > n ? n : c;
+        };
+        int zrow = tp + 1, csize = cluster_for(tp + 1);
+        {
+            int dev = 0, sms = 0;
+            RB_CUDA_TRY(cudaGetDevice(&dev));
+            RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            d.zpair = sizeof(Real) == 8 && (long long)(tp / 2) * csize >= 2LL * sms ? 1 : 0;
+        }
+        if (!d.zpair) {
+            zrow = tp;
+            csize = cluster_for(tp);
+        }
+        yz_smem = size_t((n + csize - 1) / csize) * zrow * sizeof(Real);
         d.zstaged = 1;
         if (yz_smem > size_t(kSliceBytes)) {   // the largest block exceeds a full cluster's slices
             d.zstaged = 0;
@@ -1207,9 +1454,10 @@ struct Solver final : SolverBase {
     cudaError_t yz_attr() {
         RB_CUDA_TRY(cudaFuncSetAttribute(y_kernel<Real, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(y_smem_limit())));
-        auto fn = z_kernel<Real, kZThreads, R, C>;
-        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
-        RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        for (auto fn : {z_kernel<Real, kZThreads, R, C, false>, z_kernel<Real, kZThreads, R, C, true>}) {
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        }
         return cudaSuccess;
     }
     cudaError_t set_attributes() {
@@ -1242,13 +1490,13 @@ struct Solver final : SolverBase {
 
     template <bool R, bool C>
     // the y half-step (one warp per row) and then the z half-step (a cluster
-    // per period block); two launches
+    // per z task: a period block, or a pair of them); two launches
     cudaError_t launch_yz(const Real* ys, const Real* zs, int step, int gate, cudaStream_t on = nullptr) {
         cudaStream_t st = on ? on : stream;
         y_kernel<Real, R, C><<<nby, kYThreads, size_t(kYThreads / 32) * tp * sizeof(Real), st>>>(d, ys, step, gate);
         RB_CUDA_TRY(cudaGetLastError());
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(unsigned(tp * d.csize));
+        cfg.gridDim = dim3(unsigned(z_tasks() * d.csize));   // a cluster per z task
         cfg.blockDim = dim3(kZThreads);
         cfg.dynamicSmemBytes = yz_smem;
         cfg.stream = st;
@@ -1259,7 +1507,8 @@ struct Solver final : SolverBase {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C>, d, zs, step, gate);
+        if (d.zpair) return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C, true>, d, zs, step, gate);
+        return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C, false>, d, zs, step, gate);
     }
 
     cudaError_t launch_check(int mode) {
