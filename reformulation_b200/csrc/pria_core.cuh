@@ -69,6 +69,10 @@ constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTA
 constexpr int kMaxCluster = 16;
 constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
 constexpr int kZUnroll = 8;          // z elements per thread in flight (z kernel)
+// y row values per lane in flight (y kernel): 8 in FP32, 4 in FP64 (more
+// registers per value; measured best of 4, 8, 16 for each)
+template <class Real>
+constexpr int y_chunk() { return sizeof(Real) == 4 ? 8 : 4; }
 constexpr int kYThreads = 256;       // y kernel: one warp per row, kYThreads / 32 rows per tile
 constexpr int kZThreads = 512;       // z kernel CTA
 
@@ -367,27 +371,55 @@ __device__ __forceinline__ void y_kernel_tile(const Dev<Real>& d, int tile, cons
     const bool vanilla = !Reflect && (gate & kGateVanilla);
     const bool drift = Reflect || (gate & kGateDrift);
     double acc[3] = {0.0, 0.0, 0.0};   // |dy|^2, <dx, dy>, drift
+    constexpr int kYChunk = y_chunk<Real>();
     if (g < (long long)d.tp * d.n) {    // uniform over the warp
         const int s = int(g / d.n), i = int(g - (long long)s * d.n);
         const int len = d.tp - s;
         const long long e0 = blk(d.n, d.tp, s) + (long long)i * len;
-#pragma unroll 8
-        for (int q = lane; q < len; q += 32) {
-            v[q] = ysrc[e0 + q] + d.r[e0 + q];
-            if (drift && (q & 7) == 0) prefetch_l2(d.y0 + e0 + q);   // one per 32-byte sector
-            if (Check && (q & 7) == 0) prefetch_l2(d.dxs + e0 + q);
+        // chunks of kYChunk values per lane, loaded by predicated loads with
+        // no loop around them, so each chunk is one memory round trip (an
+        // unrolled loop over the row would end in a remainder loop that waits
+        // for every load in turn)
+        for (int q0 = 0; q0 < len; q0 += 32 * kYChunk) {   // uniform over the warp
+            Real a[kYChunk], b[kYChunk];
+#pragma unroll
+            for (int u = 0; u < kYChunk; ++u) {
+                const int q = q0 + lane + 32 * u;
+                if (q < len) {
+                    a[u] = ysrc[e0 + q];
+                    b[u] = d.r[e0 + q];
+                    if (drift && (q & 7) == 0) prefetch_l2(d.y0 + e0 + q);   // one per 32-byte sector
+                    if (Check && (q & 7) == 0) prefetch_l2(d.dxs + e0 + q);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kYChunk; ++u) {
+                const int q = q0 + lane + 32 * u;
+                if (q < len) v[q] = a[u] + b[u];
+            }
         }
         __syncwarp();
         double* slot = d.thy + (long long)s * d.n + i;
         const double th = michelot_smem(v, len, double(d.k[i]), *slot);
         if (lane == 0) *slot = th;
-#pragma unroll 4
-        for (int q = lane; q < len; q += 32) {
-            {
+        for (int q0 = 0; q0 < len; q0 += 32 * kYChunk) {   // uniform over the warp
+            Real y1v[kYChunk], ydv[kYChunk], dxv[kYChunk];
+#pragma unroll
+            for (int u = 0; u < kYChunk; ++u) {
+                const int q = q0 + lane + 32 * u;
+                if (q < len) {
+                    y1v[u] = ysrc[e0 + q];
+                    ydv[u] = drift ? d.y0[e0 + q] : y1v[u];
+                    if (Check) dxv[u] = d.dxs[e0 + q];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kYChunk; ++u) {
+                const int q = q0 + lane + 32 * u;
+                if (q >= len) continue;
                 const long long e = e0 + q;
                 const Real y2 = Real(fmax(double(v[q]) - th, 0.0));
-                const Real y1 = ysrc[e];
-                const Real yd = drift ? d.y0[e] : y1;
+                const Real y1 = y1v[u], yd = ydv[u];
                 const Real ya = Reflect ? yd : y1;
                 d.yh[e] = vanilla ? y2 : lwn * (Real(2) * y2 - y1) + rwn * ya;
                 if (!Reflect && !vanilla) d.y0[e] = y1;
@@ -395,7 +427,7 @@ __device__ __forceinline__ void y_kernel_tile(const Dev<Real>& d, int tile, cons
                     if (Reflect) d.y2s[e] = y2;
                     const double dy = double(y1) - double(y2), dr = double(y1) - double(yd);
                     acc[0] += dy * dy;
-                    acc[1] += double(d.dxs[e]) * dy;
+                    acc[1] += double(dxv[u]) * dy;
                     acc[2] += dr * dr;
                 }
             }
@@ -789,10 +821,24 @@ __device__ __forceinline__ void upper_kernel_tile(const Dev<Real>& d, int tile, 
         for (int i = warp; i < d.n; i += nwarps) {
             const long long e0 = base + (long long)i * len;
             double mx = 0.0, hx = 0.0;
-            for (int q = lane; q < valid; q += 32) {
-                const double v = double(x[e0 + q]);
-                mx = fmax(mx, v);
-                hx += double(d.h[e0 + q]) * v;
+            // chunks of 8 predicated loads per lane: one round trip each
+            for (int q0 = 0; q0 < valid; q0 += 32 * 8) {   // uniform over the warp
+                Real xv[8], hv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int q = q0 + lane + 32 * u;
+                    if (q < valid) {
+                        xv[u] = x[e0 + q];
+                        hv[u] = d.h[e0 + q];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (q0 + lane + 32 * u >= valid) continue;
+                    const double v = double(xv[u]);
+                    mx = fmax(mx, v);
+                    hx += double(hv[u]) * v;
+                }
             }
             mx = warp_max(mx);
             hx = warp_sum(hx);
@@ -837,11 +883,24 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int tt = t0 + lane;
     double mn = INFINITY;
-    for (int s = warp; s < rows; s += nwarps) {
-        if (lane < tcols && tt >= s) {
-            const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
-            mn = fmin(mn, (double(d.h[e]) + double(y[e])) + double(z[e]));
+    // four rows per warp in flight (a minimum: the order does not matter)
+    for (int s0 = warp; s0 < rows; s0 += 4 * nwarps) {
+        Real hv[4], yv[4], zv[4];
+        bool in[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int s = s0 + u * nwarps;
+            in[u] = s < rows && lane < tcols && tt >= s;
+            if (in[u]) {
+                const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
+                hv[u] = d.h[e];
+                yv[u] = y[e];
+                zv[u] = z[e];
+            }
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (in[u]) mn = fmin(mn, (double(hv[u]) + double(yv[u])) + double(zv[u]));
     }
     cmin[warp][lane] = mn;
     __syncthreads();
