@@ -57,15 +57,32 @@ __device__ __forceinline__ void block_sums(double (&v)[K], double* scratch, doub
 
 // Deterministic sum of `count` rows of K doubles (row-major, stride K) by one
 // block: thread t adds rows t, t + blockDim, ... in order, then block_sums.
+// A thread's rows are loaded four at a time by predicated loads, so each
+// group of four costs one memory round trip.
 template <int K>
 __device__ __forceinline__ void reduce_rows(const double* rows, int count, double* scratch,
                                             double* out) {
+    constexpr int kRows = 4;
     double v[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = 0.0;
-    for (int r = threadIdx.x; r < count; r += blockDim.x) {
+    for (int r0 = threadIdx.x; r0 < count; r0 += kRows * blockDim.x) {
+        double t[kRows][K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) v[k] += rows[size_t(r) * K + k];
+        for (int u = 0; u < kRows; ++u) {
+            const int r = r0 + u * int(blockDim.x);
+            if (r < count) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[u][k] = rows[size_t(r) * K + k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+            if (r0 + u * int(blockDim.x) < count) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) v[k] += t[u][k];
+            }
+        }
     }
     block_sums<K>(v, scratch, out);
 }
