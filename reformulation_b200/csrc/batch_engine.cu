@@ -78,7 +78,7 @@ bq_node(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* 
         if (threadIdx.x == 0) sd = devs[w.x];
         __syncthreads();
         praq::node_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? sd.pred : sd.u2s,
-                                                     Reflect ? sd.predc : sd.u2c, step, 0, gate);
+                                                     Reflect ? sd.pred1 : sd.u2s1, step, 0, gate);
     }
 }
 
@@ -106,7 +106,7 @@ bq_lower(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int*
         __syncthreads();
         if (threadIdx.x == 0) sd = devs[w.x];
         __syncthreads();
-        praq::lower_kernel_tile<Real>(sd, w.y, sd.u2s, sd.u2c);
+        praq::lower_kernel_tile<Real>(sd, w.y, sd.u2s, sd.u2s1);
     }
 }
 
@@ -384,6 +384,7 @@ struct Engine final : EngineBase {
         p.op_steps = op_steps;
         auto s = std::make_unique<praq::Solver<Real>>();
         s->p = p;
+        s->allow_pull = false;   // the engine's kernels read slot 1 in the push layout
         const int st = s->setup(in, stream);
         if (st) return st;
         q.push_back(QInst{std::move(s)});

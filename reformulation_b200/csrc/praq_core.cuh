@@ -15,15 +15,23 @@
 //   y + eta omega (q - S r) then collapses to
 //       covering:  mu' = clip(mu + (eta omega / 2)(1 - r_i - r_j), -w, 0)
 //       packing:   a'  = clip(a  + (eta omega / 2)(r_j - r_i),      0, w)
-// * BOTH HALF-EDGE VALUES CONTIGUOUS FOR THE SCATTER.  Edges are sorted by
-//   first end (stable), so a node's first-end half-edges are one run of
-//   `pred` (slot 0 = u).  The edge kernel also writes each edge's slot-1 value
-//   (u, or w - u) into `predc` at the edge's position in second-end order, a
-//   scattered write that costs the writer no stall; the node kernel then reads
-//   its second-end half-edges as one run of `predc`.  The node kernel has no
-//   index indirection at all; the one random read left per edge is the edge
-//   kernel's read of r at both ends (an n-sized array).
-// * `pred`/`predc` hold the NEXT step's Halpern-combined dual, computed by the
+// * SLOT 1 PUSHED OR PULLED.  Edges are sorted by first end (stable), so a
+//   node's first-end half-edges are one run of `pred` (slot 0 = u).  Each
+//   edge's slot-1 value (u, or w - u) must reach its second end too, through
+//   one random access per edge, which can sit on either side:
+//   push: the edge kernel writes it to `pred1` at the edge's position in
+//   second-end order (`colpos`), and the node kernel reads its second-end
+//   half-edges as one coalesced run;
+//   pull: the edge kernel writes it to `pred1` in edge order (coalesced), and
+//   the node kernel gathers it through `colidx` (the edges in second-end
+//   order).
+//   While the edge arrays sit in L2 the scattered write is cheap and the
+//   latency-bound node kernel should not wait on a dependent gather, so push
+//   wins (n = 1e5, m = 1e6: 1.50 vs 1.54 ms per solve); once they spill to
+//   DRAM every scattered 4-byte write costs a sector read and write, and pull
+//   wins (n = 2e6, m = 2e7: 21.9 vs 33.1 ms).  The solver pulls when the edge
+//   arrays exceed twice the L2 size.
+// * `pred`/`pred1` hold the NEXT step's Halpern-combined dual, computed by the
 //   edge kernel as it finishes a step (as the reference does), so a reflected
 //   step streams one real per edge of dual state plus the anchor.
 // * Every decision of _halpern_step (restart tests, omega/theta update,
@@ -49,6 +57,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -93,16 +102,18 @@ struct Dev {
     int n, m;
     const int* row_ptr;    // [n+1] first-end runs in sorted edge order
     const int* col_ptr;    // [n+1] second-end runs in second-end order
-    const int* colpos;     // [m] position of sorted edge s in second-end order
+    int pull;              // slot-1 layout: 1 pull (edge order), 0 push (second-end order)
+    const int* colidx;     // [m] pull: the sorted edge at position k of second-end order
+    const int* colpos;     // [m] push: the second-end position of sorted edge s
     const int2* ends;      // [m]
     const Real* w;         // [m] signed, 2 W_ij / scale
     const Real* diag;      // [n] W_ii / scale
     const Real* deg;       // [n] incident half-edges, floored at 1
     const double* scale;   // [1] objective scale
     Real *x1, *x2, *x0, *r;
-    Real *pred, *predc;    // next combined dual: slot 0 (sorted order), slot 1 (second-end order)
+    Real *pred, *pred1;    // next combined dual: slot 0 (sorted edge order) and slot 1 (by layout)
     Real *u0;              // anchor (sorted order)
-    Real *u2s, *u2c;       // y2 at the last check, in the two orders
+    Real *u2s, *u2s1;      // y2 at the last check: slot 0 and slot 1, as pred and pred1
     double *pnode, *pedge, *plower;
     Control* ctl;
 };
@@ -114,11 +125,15 @@ __device__ __forceinline__ bool skip(const Control* c, int gate) {
 #ifndef RB200_PRAQ_STAGE_BYTES
 #define RB200_PRAQ_STAGE_BYTES 2048   // per warp, run and pass; compile-time tunable (sweeps build with -D)
 #endif
+#ifndef RB200_PRAQ_PULL
+#define RB200_PRAQ_PULL 2   // slot-1 layout: 0 push, 1 pull, 2 by size
+#endif
 #ifndef RB200_PRAQ_GATHER
 #define RB200_PRAQ_GATHER 2   // node gather: 0 one run after the other, 1 both at once, 2 by grid size
 #endif
 constexpr int kSeqChunk = 4;   // sequential gather: loads per lane in flight
 constexpr int kGather = RB200_PRAQ_GATHER;
+constexpr int kPull = RB200_PRAQ_PULL;
 // half-edge values a warp stages per run and pass
 template <class Real>
 constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
@@ -132,9 +147,10 @@ constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 // waves, where the issue rate, not the latency of one warp, bounds the kernel
 // (chunks of 4 loads per lane: 2 % faster per solve at n >= 1.5e5 than an
 // unrolled loop; 8 were no better).
-template <class Real, class Acc>
-__device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v, int n,
-                                         long long base, int lane, Real* __restrict__ stage) {
+template <class Real, class Acc, bool Indexed>
+__device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v,
+                                         const int* __restrict__ idx, int n, long long base, int lane,
+                                         Real* __restrict__ stage) {
     if (base >= n) return Acc(0);   // uniform over the warp
     const long long i = base + lane;
     const long long last = base + 32 < n ? base + 32 : n;
@@ -153,10 +169,24 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
         // remainder loop that waits for each load in turn)
         for (int k0 = c0; k0 < c1; k0 += 32 * kSeqChunk) {
             Real t[kSeqChunk];
+            if constexpr (Indexed) {   // value k is v[idx[k]]
+                int at[kSeqChunk];
 #pragma unroll
-            for (int u = 0; u < kSeqChunk; ++u) {
-                const int k = k0 + lane + 32 * u;
-                if (k < c1) t[u] = v[k];
+                for (int u = 0; u < kSeqChunk; ++u) {
+                    const int k = k0 + lane + 32 * u;
+                    if (k < c1) at[u] = idx[k];
+                }
+#pragma unroll
+                for (int u = 0; u < kSeqChunk; ++u) {
+                    const int k = k0 + lane + 32 * u;
+                    if (k < c1) t[u] = v[at[u]];
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < kSeqChunk; ++u) {
+                    const int k = k0 + lane + 32 * u;
+                    if (k < c1) t[u] = v[k];
+                }
             }
 #pragma unroll
             for (int u = 0; u < kSeqChunk; ++u) {
@@ -174,20 +204,22 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
 
 // The sums, for the 32 consecutive nodes i = base + lane of a warp (one node
 // per lane), of two runs at once: run a = va[pa[i] .. pa[i+1]) and run b =
-// vb[pb[i] .. pb[i+1]).  The warp copies the ranges va[pa[base] .. pa[base+32])
-// and vb[pb[base] .. pb[base+32]) through shared memory in coalesced passes of
-// kStage values each, and every lane adds its own runs' parts of each pass in
-// order.  A pass's loads, of both ranges, are predicated loads into registers
+// vb[k] (IndexB: vb[ib[k]]) for k in [pb[i], pb[i+1]).  The warp copies the
+// ranges of both runs for its 32 nodes through shared memory in passes of
+// kStage values each (run a and run b, or run b's indices, coalesced; with
+// IndexB run b's values gathered), and every lane adds its own runs' parts of
+// each pass in order.  A pass's loads, of both ranges, are predicated loads into registers
 // with no loop around them, so all of them are in flight together: one memory
 // round trip per pass (a warp-uniform exit skips the slots past both ranges).
 // The sums are those of warp_runs, term for term and in the same order.
 // Twice the registers of warp_runs: the form for grids of one wave, which the
 // latency of a warp's dependent loads bounds.  All lanes of the warp must call
 // it with the same base.
-template <class Real, class Acc>
+template <class Real, class Acc, bool IndexB>
 __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Real* __restrict__ va,
                                            const int* __restrict__ pb, const Real* __restrict__ vb,
-                                           int n, long long base, int lane, Real* __restrict__ sa,
+                                           const int* __restrict__ ib, int n, long long base, int lane,
+                                           Real* __restrict__ sa,
                                            Real* __restrict__ sb, Acc& ra, Acc& rb) {
     ra = Acc(0);
     rb = Acc(0);
@@ -210,21 +242,50 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
         // lane-relative bases and counts, so each load is a base plus an
         // immediate offset
         const Real* __restrict__ ga = va + (ca + lane);
-        const Real* __restrict__ gb = vb + (cb + lane);
         const int na = ea - ca - lane, nb = eb - cb - lane;
         const int wide = max(ea - ca, eb - cb);   // the same on every lane
-        Real ta[kPer], tb[kPer];
+        if constexpr (IndexB) {
+            const int* __restrict__ gib = ib + (cb + lane);
+            Real ta[kPer];
+            int at[kPer];
 #pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            if (32 * q >= wide) break;
-            if (32 * q < na) ta[q] = ga[32 * q];
-            if (32 * q < nb) tb[q] = gb[32 * q];
-        }
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < na) ta[q] = ga[32 * q];
+                if (32 * q < nb) at[q] = gib[32 * q];
+            }
+            // run a to shared memory first, so its registers are free before
+            // the gather of run b is issued
 #pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            if (32 * q >= wide) break;
-            if (32 * q < na) sa[lane + 32 * q] = ta[q];
-            if (32 * q < nb) sb[lane + 32 * q] = tb[q];
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < na) sa[lane + 32 * q] = ta[q];
+            }
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < nb) ta[q] = vb[at[q]];
+            }
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < nb) sb[lane + 32 * q] = ta[q];
+            }
+        } else {
+            const Real* __restrict__ gb = vb + (cb + lane);
+            Real ta[kPer], tb[kPer];
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < na) ta[q] = ga[32 * q];
+                if (32 * q < nb) tb[q] = gb[32 * q];
+            }
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (32 * q >= wide) break;
+                if (32 * q < na) sa[lane + 32 * q] = ta[q];
+                if (32 * q < nb) sb[lane + 32 * q] = tb[q];
+            }
         }
         __syncwarp();
         for (int k = max(a0, ca), e = min(a1, ea); k < e; ++k) ra += Acc(sa[k - ca]);
@@ -233,24 +294,26 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
     }
 }
 
-// S^T y at node base + lane: the node's run of `ys` (first-end order) plus its
-// run of `yc` (second-end order).  `stage` holds stage_runs<Wide> * stage_len
-// values; both forms give the same sum.
+// S^T y at node base + lane: the node's run of `ys` (slot 0, first-end order)
+// plus its run of slot-1 values of `yc`: in the push layout `yc` is in
+// second-end order, in the pull layout it is in edge order and read through
+// d.colidx (second-end order).  `stage` holds stage_runs<Wide> * stage_len
+// values; all forms give the same sum.
 template <bool Wide>
 constexpr int stage_runs() { return Wide ? 2 : 1; }
 
-template <class Real, class Acc, bool Wide>
+template <class Real, class Acc, bool Wide, bool Pull>
 __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __restrict__ ys,
                                           const Real* __restrict__ yc, long long base, int lane,
                                           Real* __restrict__ stage) {
     if constexpr (Wide) {
         Acc s0, s1;
-        warp_runs2<Real, Acc>(d.row_ptr, ys, d.col_ptr, yc, d.n, base, lane, stage,
-                              stage + stage_len<Real>(), s0, s1);
+        warp_runs2<Real, Acc, Pull>(d.row_ptr, ys, d.col_ptr, yc, d.colidx, d.n, base, lane, stage,
+                                    stage + stage_len<Real>(), s0, s1);
         return s0 + s1;
     } else {
-        const Acc s0 = warp_runs<Real, Acc>(d.row_ptr, ys, d.n, base, lane, stage);
-        const Acc s1 = warp_runs<Real, Acc>(d.col_ptr, yc, d.n, base, lane, stage);
+        const Acc s0 = warp_runs<Real, Acc, false>(d.row_ptr, ys, nullptr, d.n, base, lane, stage);
+        const Acc s1 = warp_runs<Real, Acc, Pull>(d.col_ptr, yc, d.colidx, d.n, base, lane, stage);
         return s0 + s1;
     }
 }
@@ -259,7 +322,7 @@ __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __rest
 // (solver.py:259-267 and 276-292).  Reflect: x1 = lw (2 x2 - x1) + rw x0 with
 // k = restart_iter + step + 1; vanilla: x1 = x2 and the anchor becomes x1.
 // Check: the node sums of this step go to pnode.
-template <class Real, bool Reflect, bool Check, bool Wide = false>
+template <class Real, bool Reflect, bool Check, bool Wide = false, bool Pull = false>
 __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
             int bounds_at_1, int gate) {
     const Control* c = d.ctl;
@@ -281,7 +344,7 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
             x0o = d.x0[i];
         }
     }
-    const Real s = scatter_at<Real, Real, Wide>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const Real s = scatter_at<Real, Real, Wide, Pull>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[kNodeSums] = {0.0, 0.0, 0.0};
     if (owner) {
         Real x1v;
@@ -314,20 +377,20 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
     }
 }
 
-template <class Real, bool Reflect, bool Check, bool Wide = false>
+template <class Real, bool Reflect, bool Check, bool Wide = false, bool Pull = false>
 __global__ void __launch_bounds__(kBlock)
 node_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
             int bounds_at_1, int gate) {
     pdl_wait();
     pdl_launch_dependents();
-    node_kernel_tile<Real, Reflect, Check, Wide>(d, blockIdx.x, ys, yc, step, bounds_at_1, gate);
+    node_kernel_tile<Real, Reflect, Check, Wide, Pull>(d, blockIdx.x, ys, yc, step, bounds_at_1, gate);
 }
 
 // Dual half of one PDHG step (solver.py:269-273, projection.py:16-42) in the
 // one-coordinate form, plus the prediction of the next step's combined dual.
 // Each thread takes kEdgesPerThread edges a block-stride apart, so all their
 // loads are in flight together.
-template <class Real, bool Reflect, bool Check>
+template <class Real, bool Reflect, bool Check, bool Pull = false>
 __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, const Real* ysrc, int step, int bounds_at_1, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
@@ -338,7 +401,7 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
     int2 ij[kEdgesPerThread];
     Real sw[kEdgesPerThread], u1[kEdgesPerThread], u0[kEdgesPerThread];
-    int cp[kEdgesPerThread];
+    int at1[kEdgesPerThread];   // where slot 1 goes: the edge (pull) or its second-end position (push)
 #pragma unroll
     for (int t = 0; t < kEdgesPerThread; ++t) {
         const int e = base + t * kBlock;
@@ -347,7 +410,7 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
             sw[t] = d.w[e];
             u1[t] = Reflect ? d.pred[e] : ysrc[e];
             u0[t] = Reflect ? d.u0[e] : u1[t];
-            cp[t] = d.colpos[e];
+            at1[t] = Pull ? e : d.colpos[e];
         }
     }
     Real ri[kEdgesPerThread], rj[kEdgesPerThread];
@@ -369,12 +432,12 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
                             : clampv(u1[t] + hs * (rj[t] - ri[t]), Real(0), w);
         const Real nx = lwn * (Real(2) * u2 - u1[t]) + rwn * u0[t];
         d.pred[e] = nx;
-        d.predc[cp[t]] = cov ? nx : w - nx;
+        d.pred1[at1[t]] = cov ? nx : w - nx;
         if (!Reflect) d.u0[e] = u1[t];
         if (Check) {
             if (Reflect) {
                 d.u2s[e] = u2;
-                d.u2c[cp[t]] = cov ? u2 : w - u2;
+                d.u2s1[at1[t]] = cov ? u2 : w - u2;
             }
             const double x1i = d.x1[ij[t].x], x2i = d.x2[ij[t].x];
             const double x1j = d.x1[ij[t].y], x2j = d.x2[ij[t].y];
@@ -398,17 +461,17 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
     }
 }
 
-template <class Real, bool Reflect, bool Check>
+template <class Real, bool Reflect, bool Check, bool Pull = false>
 __global__ void __launch_bounds__(kBlock)
 edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) {
     pdl_wait();
     pdl_launch_dependents();
-    edge_kernel_tile<Real, Reflect, Check>(d, blockIdx.x, ysrc, step, bounds_at_1, gate);
+    edge_kernel_tile<Real, Reflect, Check, Pull>(d, blockIdx.x, ysrc, step, bounds_at_1, gate);
 }
 
 // The node part of the lower bound, sum_i min(d_i - (S^T y)_i, 0), at the
 // dual (ys, yc) (solver.py:333-337), in FP64.
-template <class Real, bool Wide = false>
+template <class Real, bool Wide = false, bool Pull = false>
 __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     if (d.ctl->terminated) return;
     __shared__ double scratch[32];
@@ -416,7 +479,7 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
-    const double s = scatter_at<Real, double, Wide>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const double s = scatter_at<Real, double, Wide, Pull>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
     double acc[1] = {0.0};
     if (i < d.n) {
         const double rc = double(d.diag[i]) - s;
@@ -426,12 +489,12 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
     if (threadIdx.x == 0) d.plower[tile] = acc[0];
 }
 
-template <class Real, bool Wide = false>
+template <class Real, bool Wide = false, bool Pull = false>
 __global__ void __launch_bounds__(kBlock)
 lower_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ yc) {
     pdl_wait();
     pdl_launch_dependents();
-    lower_kernel_tile<Real, Wide>(d, blockIdx.x, ys, yc);
+    lower_kernel_tile<Real, Wide, Pull>(d, blockIdx.x, ys, yc);
 }
 
 __device__ __forceinline__ double canonical(const double* node, const double* edge, double omega) {
@@ -537,8 +600,9 @@ __global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta)
         d.u0[k] = u;
         d.pred[k] = u;
         d.u2s[k] = u;
-        d.predc[d.colpos[k]] = v;
-        d.u2c[d.colpos[k]] = v;
+        const long long at = d.pull ? k : d.colpos[k];
+        d.pred1[at] = v;
+        d.u2s1[at] = v;
     }
     if (k == 0) {
         c->omega = omega;
@@ -586,8 +650,9 @@ __global__ void warm_init_kernel(Dev<Real> d, Control* c, double omega, double t
         d.u0[k] = u;
         d.pred[k] = u;
         d.u2s[k] = u;
-        d.predc[d.colpos[k]] = v;
-        d.u2c[d.colpos[k]] = v;
+        const long long at = d.pull ? k : d.colpos[k];
+        d.pred1[at] = v;
+        d.u2s1[at] = v;
     }
     if (k == 0) {
         c->omega = omega;
@@ -715,9 +780,9 @@ struct Solver final : SolverBase {
     PraqParameters p{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    PoolBuf<int> row_ptr, col_ptr, colpos, perm;
+    PoolBuf<int> row_ptr, col_ptr, colidx, colpos, perm;
     PoolBuf<int2> ends;
-    PoolBuf<Real> w, diag, deg, x1, x2, x0, r, pred, predc, u0, u2s, u2c;
+    PoolBuf<Real> w, diag, deg, x1, x2, x0, r, pred, pred1, u0, u2s, u2s1;
     PoolBuf<double> pnode, pedge, plower, scale;
     PoolBuf<double> warm_x, warm_y;   // a warm start (instance units), optional
     PoolBuf<Control> ctl;
@@ -725,6 +790,8 @@ struct Solver final : SolverBase {
     Dev<Real> d{};
     int nb_node = 1, nb_edge = 1;
     bool wide = false;   // node gather of both runs at once (warp_runs2)
+    bool pull = false;   // slot-1 layout (see the layout notes at the top)
+    bool allow_pull = true;   // false: always push (the batched engine's kernels)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
@@ -738,10 +805,11 @@ struct Solver final : SolverBase {
         if (graph) cudaGraphDestroy(graph);
         for (auto& ev : done) if (ev) cudaEventDestroy(ev);
         for (auto& ev : evpool) cudaEventDestroy(ev);
-        row_ptr.release(); col_ptr.release(); colpos.release(); perm.release(); ends.release();
+        row_ptr.release(); col_ptr.release(); colidx.release(); colpos.release(); perm.release();
+        ends.release();
         w.release(); diag.release(); deg.release();
-        x1.release(); x2.release(); x0.release(); r.release(); pred.release(); predc.release();
-        u0.release(); u2s.release(); u2c.release();
+        x1.release(); x2.release(); x0.release(); r.release(); pred.release(); pred1.release();
+        u0.release(); u2s.release(); u2s1.release();
         pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release();
         warm_x.release(); warm_y.release();
         if (stream) cudaStreamSynchronize(stream);
@@ -761,6 +829,7 @@ struct Solver final : SolverBase {
         }
         mirror = static_cast<Control*>(pinned_get());
         if (!mirror) return PRAQ_ERROR_CUDA;
+        pull = choose_pull(in.m);
         const int st = layout(in);
         if (st) return st;
         nb_node = ceil_div(n, kBlock);   // one node per thread
@@ -777,7 +846,7 @@ struct Solver final : SolverBase {
         }
         for (auto* b : {&x1, &x2, &x0, &r})
             if (b->alloc(n, stream)) return PRAQ_ERROR_CUDA;
-        for (auto* b : {&pred, &predc, &u0, &u2s, &u2c})
+        for (auto* b : {&pred, &pred1, &u0, &u2s, &u2s1})
             if (b->alloc(m, stream)) return PRAQ_ERROR_CUDA;
         if (pnode.alloc(size_t(nb_node) * kNodeSums, stream) ||
             pedge.alloc(size_t(nb_edge) * kEdgeSums, stream) || plower.alloc(nb_node, stream) ||
@@ -792,10 +861,13 @@ struct Solver final : SolverBase {
         for (auto& ev : done)
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return PRAQ_ERROR_CUDA;
         d.n = n; d.m = m;
-        d.row_ptr = row_ptr.ptr; d.col_ptr = col_ptr.ptr; d.colpos = colpos.ptr;
+        d.row_ptr = row_ptr.ptr; d.col_ptr = col_ptr.ptr;
+        d.pull = pull ? 1 : 0;
+        d.colidx = pull ? colidx.ptr : nullptr;
+        d.colpos = pull ? nullptr : colpos.ptr;
         d.ends = ends.ptr; d.w = w.ptr; d.diag = diag.ptr; d.deg = deg.ptr; d.scale = scale.ptr;
         d.x1 = x1.ptr; d.x2 = x2.ptr; d.x0 = x0.ptr; d.r = r.ptr;
-        d.pred = pred.ptr; d.predc = predc.ptr; d.u0 = u0.ptr; d.u2s = u2s.ptr; d.u2c = u2c.ptr;
+        d.pred = pred.ptr; d.pred1 = pred1.ptr; d.u0 = u0.ptr; d.u2s = u2s.ptr; d.u2s1 = u2s1.ptr;
         d.pnode = pnode.ptr; d.pedge = pedge.ptr; d.plower = plower.ptr; d.ctl = ctl.ptr;
         prm.tolerance = p.tolerance;
         prm.max_iter = p.max_iter;
@@ -814,7 +886,7 @@ struct Solver final : SolverBase {
         m = int(in.m);
         PoolBuf<int64_t> rows, cols;
         PoolBuf<double> vals, dg, part;
-        PoolBuf<int> krow, kcol, first, second, sidx, flags, keys2, order2, iota, ksorted;
+        PoolBuf<int> krow, kcol, first, second, sidx, flags, keys2, iota, ksorted;
         PoolBuf<unsigned char> temp;
         if (dg.upload(in.diag, n, stream) || rows.upload(in.rows, m, stream) ||
             cols.upload(in.cols, m, stream) || vals.upload(in.vals, m, stream) ||
@@ -834,8 +906,8 @@ struct Solver final : SolverBase {
         if (fl & 1) return PRAQ_ERROR_INSTANCE;
         if (ends.alloc(m, stream) || w.alloc(m, stream) || first.alloc(m, stream) ||
             second.alloc(m, stream) || sidx.alloc(m, stream) || row_ptr.alloc(n + 1, stream) ||
-            col_ptr.alloc(n + 1, stream) || colpos.alloc(m, stream) || diag.alloc(n, stream) ||
-            deg.alloc(n, stream) || keys2.alloc(m, stream) || order2.alloc(m, stream))
+            col_ptr.alloc(n + 1, stream) || colidx.alloc(m, stream) || diag.alloc(n, stream) ||
+            deg.alloc(n, stream) || keys2.alloc(m, stream))
             return PRAQ_ERROR_CUDA;
         int key_bits = 1;
         while (key_bits < 31 && (1LL << key_bits) < (long long)n) ++key_bits;
@@ -862,8 +934,12 @@ struct Solver final : SolverBase {
                 m, permp, krow.ptr, kcol.ptr, vals.ptr, scale.ptr, ends.ptr, w.ptr, first.ptr,
                 second.ptr, sidx.ptr);
             // second-end order: a stable sort of the sorted edges by second end
-            if (radix(second.ptr, keys2.ptr, sidx.ptr, order2.ptr)) return PRAQ_ERROR_CUDA;
-            prep_colpos_kernel<<<ceil_div(m, kBlock), kBlock, 0, stream>>>(m, order2.ptr, colpos.ptr);
+            if (radix(second.ptr, keys2.ptr, sidx.ptr, colidx.ptr)) return PRAQ_ERROR_CUDA;
+            if (!pull) {   // push: the inverse permutation, and no index afterwards
+                if (colpos.alloc(m, stream)) return PRAQ_ERROR_CUDA;
+                prep_colpos_kernel<<<ceil_div(m, kBlock), kBlock, 0, stream>>>(m, colidx.ptr, colpos.ptr);
+                colidx.release();
+            }
         }
         prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, first.ptr, row_ptr.ptr);
         prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, keys2.ptr, col_ptr.ptr);
@@ -904,25 +980,28 @@ struct Solver final : SolverBase {
     // One op_steps block: op_steps reflected steps (the last with the check
     // sums), the lower-bound pass, the check, then the restart step (gated on
     // the device flag), its error, and a copy of the control block to the host.
-    cudaError_t enqueue_block() { return wide ? enqueue_steps<true>() : enqueue_steps<false>(); }
+    cudaError_t enqueue_block() {
+        if (pull) return wide ? enqueue_steps<true, true>() : enqueue_steps<false, true>();
+        return wide ? enqueue_steps<true, false>() : enqueue_steps<false, false>();
+    }
 
-    template <bool W>
+    template <bool W, bool P>
     cudaError_t enqueue_steps() {
         const int op = int(p.op_steps);
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
-                RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false, W>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
-                if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, false>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
+                RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false, W, P>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.pred1, s, 0, 0)));
+                if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, false, P>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             } else {
-                RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true, W>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.predc, s, 0, 0)));
-                if (m) RB_TIMED(3, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, true>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
+                RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true, W, P>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.pred1, s, 0, 0)));
+                if (m) RB_TIMED(3, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, true, P>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             }
         }
-        RB_TIMED(4, RB_CUDA_TRY(launch_pdl(lower_kernel<Real, W>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c)));
+        RB_TIMED(4, RB_CUDA_TRY(launch_pdl(lower_kernel<Real, W, P>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2s1)));
         RB_TIMED(5, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 1)));
-        RB_TIMED(6, RB_CUDA_TRY(launch_pdl(node_kernel<Real, false, true, W>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2c, 0, 0, 1)));
-        if (m) RB_TIMED(7, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, false, true>, nb_edge, kBlock, stream, d, (const Real*)d.u2s, 0, 0, 1)));
+        RB_TIMED(6, RB_CUDA_TRY(launch_pdl(node_kernel<Real, false, true, W, P>, nb_node, kBlock, stream, d, (const Real*)d.u2s, (const Real*)d.u2s1, 0, 0, 1)));
+        if (m) RB_TIMED(7, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, false, true, P>, nb_edge, kBlock, stream, d, (const Real*)d.u2s, 0, 0, 1)));
         RB_TIMED(8, RB_CUDA_TRY(launch_pdl(check_kernel, 1, kCheckBlock, stream, d.ctl, prm, (const double*)d.scale, (const double*)d.pnode, nb_node,
                                                                 d.pedge, nb_edge, d.plower, nb_node, 2)));
         RB_CUDA_TRY(cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
@@ -951,6 +1030,30 @@ struct Solver final : SolverBase {
         return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
     }
 
+    // x1, y1 = _raw_step(x0, y0): one vanilla step from the start, with the
+    // sums for the error and the bounds at the start point
+    template <bool P>
+    void start_step() {
+        node_kernel<Real, false, true, false, P><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.pred1, 0, 1, 0);
+        lower_kernel<Real, false, P><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.pred1);
+        if (m) edge_kernel<Real, false, true, P><<<nb_edge, kBlock, 0, stream>>>(d, d.pred, 0, 1, 0);
+    }
+
+    // Slot-1 layout for m edges: pull once the step's edge arrays (ends, w,
+    // pred, pred1, u0 and the index: 12 + 4 R bytes per edge) exceed twice the
+    // L2 size.  REFORM_PRAQ_SLOT1=push|pull in the environment overrides the
+    // choice (for tests and measurements).
+    bool choose_pull(int64_t m_) const {
+        if (!allow_pull) return false;
+        const char* env = std::getenv("REFORM_PRAQ_SLOT1");
+        if (env && !std::strcmp(env, "push")) return false;
+        if (env && !std::strcmp(env, "pull")) return true;
+        if (kPull != 2) return kPull == 1;
+        int dev = 0, l2 = 0;
+        if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev)) return false;
+        return double(m_) * (12.0 + 4.0 * sizeof(Real)) > 2.0 * double(l2);
+    }
+
     // Cold (or warm) start, the first vanilla step and the check before the loop.
     int start_solve() {
         nlaunch = 0;
@@ -962,9 +1065,8 @@ struct Solver final : SolverBase {
             init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
         // x1, y1 = _raw_step(x0, y0): one vanilla step from the start, with
         // the sums for the error and the bounds at the start point.
-        node_kernel<Real, false, true><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc, 0, 1, 0);
-        lower_kernel<Real><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.predc);
-        if (m) edge_kernel<Real, false, true><<<nb_edge, kBlock, 0, stream>>>(d, d.pred, 0, 1, 0);
+        if (pull) start_step<true>();
+        else start_step<false>();
         check_kernel<<<1, kCheckBlock, 0, stream>>>(d.ctl, prm, d.scale, d.pnode, nb_node, d.pedge, nb_edge,
                                                    d.plower, nb_node, 0);
         if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
@@ -1095,9 +1197,9 @@ struct Solver final : SolverBase {
 
     size_t device_bytes() const {
         size_t b = 0;
-        b += (row_ptr.count + col_ptr.count + colpos.count + perm.count) * sizeof(int);
+        b += (row_ptr.count + col_ptr.count + colidx.count + colpos.count + perm.count) * sizeof(int);
         b += ends.count * sizeof(int2);
-        for (auto* x : {&w, &diag, &deg, &x1, &x2, &x0, &r, &pred, &predc, &u0, &u2s, &u2c})
+        for (auto* x : {&w, &diag, &deg, &x1, &x2, &x0, &r, &pred, &pred1, &u0, &u2s, &u2s1})
             b += x->count * sizeof(Real);
         for (auto* x : {&pnode, &pedge, &plower, &scale}) b += x->count * sizeof(double);
         return b + sizeof(Control);

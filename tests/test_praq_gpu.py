@@ -240,3 +240,39 @@ def test_edgeless_instance_terminates(lib):
     for _ in range(3):
         s = lib.solve(inst, lib.parameters(tolerance=1e-9, max_iter=10_000))
         assert s.status == 0 and abs(s.upper - (-3.0)) <= 1e-8
+
+
+@pytest.mark.parametrize("use_float32", [0, 1])
+def test_slot1_layouts_agree(native, oracle_lib, monkeypatch, use_float32):
+    """The two slot-1 layouts (push: scattered by the edge kernel; pull:
+    gathered by the node kernel through the second-end index) add the same
+    values in the same order, so a solve, its dual and a warm-started solve
+    agree bit for bit; the pull layout also meets the max-flow roof dual.
+    Unsorted, flipped edges exercise the warm start's edge permutation."""
+    from reformulation_b200.praq import DeviceSolver, Library
+    base = random_qubo(11, 500, 0.05)
+    rng = np.random.default_rng(5)
+    order = rng.permutation(base.edges)
+    flip = rng.random(base.edges) < 0.5
+    rows, cols = base.rows[order].copy(), base.cols[order].copy()
+    rows[flip], cols[flip] = cols[flip], rows[flip].copy()
+    inst = QuboInstance("s", "s", base.n, base.diag, rows, cols, base.vals[order])
+    tol = 1e-4 if use_float32 else 1e-9
+    p = Library().parameters(tolerance=tol, use_float32=use_float32)
+    out = {}
+    for layout in ("push", "pull"):
+        monkeypatch.setenv("REFORM_PRAQ_SLOT1", layout)
+        with DeviceSolver(inst, p) as dev:
+            assert dev.run() == 0
+            res, y = dev.result(want_x=True, want_dual=True)
+            dev.set_warm(0.5 * (res.x + 0.5), y)
+            assert dev.run() == 0
+            warm = dev.result(want_x=True)
+        out[layout] = (res, y, warm)
+    (a, ya, wa), (b, yb, wb) = out["push"], out["pull"]
+    assert (a.iterations, a.lower, a.upper) == (b.iterations, b.lower, b.upper)
+    assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
+    assert (wa.iterations, wa.lower, wa.upper) == (wb.iterations, wb.lower, wb.upper)
+    assert np.array_equal(wa.x, wb.x)
+    if not use_float32:
+        assert rel(b.upper, oracle_lib.roof_dual_maxflow(base)) <= 1e-7
