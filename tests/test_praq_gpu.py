@@ -276,3 +276,23 @@ def test_slot1_layouts_agree(native, oracle_lib, monkeypatch, use_float32):
     assert np.array_equal(wa.x, wb.x)
     if not use_float32:
         assert rel(b.upper, oracle_lib.roof_dual_maxflow(base)) <= 1e-7
+
+
+@pytest.mark.parametrize("use_float32", [0, 1])
+def test_slot1_layouts_agree_sequential_gather(native, monkeypatch, use_float32):
+    """The same agreement with the node grid past one wave (n = 150,000), where
+    the solver takes the sequential node gather: both layouts, bit for bit."""
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = qubo_uniform_edges(3, 150_000, 300_000)
+    p = Library().parameters(tolerance=1e-4, use_float32=use_float32, max_iter=200)
+    out = {}
+    for layout in ("push", "pull"):
+        monkeypatch.setenv("REFORM_PRAQ_SLOT1", layout)
+        with DeviceSolver(inst, p) as dev:
+            dev.run()
+            out[layout] = dev.result(want_x=True, want_dual=True)
+    (a, ya), (b, yb) = out["push"], out["pull"]
+    assert (a.status, a.iterations, a.lower, a.upper) == (b.status, b.iterations, b.lower, b.upper)
+    assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
+    assert a.lower <= a.upper
