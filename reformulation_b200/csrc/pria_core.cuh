@@ -47,6 +47,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -1448,6 +1449,9 @@ struct Solver final : SolverBase {
             RB_CUDA_TRY(cudaGetDevice(&dev));
             RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             d.zpair = sizeof(Real) == 8 && (long long)(tp / 2) * csize >= 2LL * sms ? 1 : 0;
+            // REFORM_PRIA_ZPAIR=0|1 overrides the choice (tests, measurements)
+            const char* env = std::getenv("REFORM_PRIA_ZPAIR");
+            if (env && (env[0] == '0' || env[0] == '1') && env[1] == '\0') d.zpair = env[0] - '0';
         }
         if (!d.zpair) {
             zrow = tp;

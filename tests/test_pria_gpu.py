@@ -242,3 +242,26 @@ def test_block_beyond_cluster_shared_memory(native):
     assert ra.dual_objective <= ra.primal_objective
     assert rel(ra.primal_objective, rb.primal_objective) <= 1e-3
     assert rel(ra.dual_objective, rb.dual_objective) <= 1e-3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(30, 400), (8, 300)])
+def test_z_block_pairs_equal_single_blocks(native, monkeypatch, precision, shape):
+    """The z half-step in pairs of period blocks (s, Tp - 1 - s) per cluster,
+    the solver's choice in FP64 on large grids, adds every per-block sum in
+    the order of one block per cluster: the same solve with either gives the
+    same iterations, objectives and x, y, z bit for bit."""
+    from reformulation_b200 import pria
+    inst = jrp_demand(12, shape[0], shape[1])
+    p = pria.Library().parameters(-1, 1e-6)
+    out = {}
+    for pair in ("0", "1"):
+        monkeypatch.setenv("REFORM_PRIA_ZPAIR", pair)
+        with pria.DeviceSolver(inst, p, precision) as dev:
+            assert dev.run() == 0
+            out[pair] = dev.result(want_solution=True)
+    a, b = out["0"], out["1"]
+    assert a.iterations == b.iterations
+    assert a.primal_objective == b.primal_objective and a.dual_objective == b.dual_objective
+    for k in ("x", "y", "z"):
+        assert np.array_equal(getattr(a, k), getattr(b, k))
