@@ -1,8 +1,13 @@
 // memory.cu -- the pools declared in memory.cuh.
 #include "memory.cuh"
 
+#include <algorithm>
+#include <condition_variable>
 #include <cstdint>
+#include <cstring>
+#include <functional>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace rb200 {
@@ -63,6 +68,123 @@ void pinned_put(void* slot) {
     if (!slot) return;
     std::lock_guard<std::mutex> lock(slab_mu);
     slab_free.push_back(int((static_cast<char*>(slot) - slab_base) / kSlot));
+}
+
+}  // namespace rb200
+
+// --- staged host-to-device copies ---------------------------------------------
+
+namespace rb200 {
+namespace {
+
+// A fixed set of host threads that run one job at a time: parallel(f) calls
+// f(k) for k = 0 .. size-1, k = 0 on the calling thread, and returns when all
+// have returned.  Started on first use, joined at exit.
+class HostThreads {
+public:
+    explicit HostThreads(int helpers) : helpers_(helpers) {
+        for (int k = 1; k <= helpers_; ++k) threads_.emplace_back([this, k] { loop(k); });
+    }
+    ~HostThreads() {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            stop_ = true;
+        }
+        wake_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    int size() const { return helpers_ + 1; }
+    void parallel(const std::function<void(int)>& f) {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            job_ = &f;
+            pending_ = helpers_;
+            ++generation_;
+        }
+        wake_.notify_all();
+        f(0);
+        std::unique_lock<std::mutex> lock(mu_);
+        done_.wait(lock, [this] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+private:
+    void loop(int k) {
+        long long seen = 0;
+        for (;;) {
+            const std::function<void(int)>* f;
+            {
+                std::unique_lock<std::mutex> lock(mu_);
+                wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
+                if (stop_) return;
+                seen = generation_;
+                f = job_;
+            }
+            (*f)(k);
+            std::lock_guard<std::mutex> lock(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    int helpers_;
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable wake_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    long long generation_ = 0;
+    int pending_ = 0;
+    bool stop_ = false;
+};
+
+HostThreads& host_threads() {
+    static HostThreads pool(std::max(0, std::min(7, int(std::thread::hardware_concurrency()) - 1)));
+    return pool;
+}
+
+constexpr size_t kStageBytes = size_t(4) << 20;   // per slot; two slots
+std::mutex stage_mu;
+char* stage_ring = nullptr;
+cudaEvent_t stage_done[64][2] = {};                 // per device and slot
+int stage_dev[2] = {-1, -1};                        // the device whose copy last read each slot
+
+// Copies `bytes` of output to dst in chunks: fill(chunk_dst_host, first_byte,
+// chunk_bytes) writes a chunk into a pinned slot, split over the host threads.
+template <class Fill>
+cudaError_t staged(char* dst, size_t bytes, size_t unit, cudaStream_t stream, Fill fill) {
+    if (!bytes) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(stage_mu);
+    int dev = 0;
+    RB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!stage_ring) RB_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&stage_ring), 2 * kStageBytes,
+                                               cudaHostAllocPortable));
+    for (auto& ev : stage_done[dev])
+        if (!ev) RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    HostThreads& pool = host_threads();
+    const size_t chunk = kStageBytes / unit * unit;
+    int slot = 0;
+    for (size_t off = 0; off < bytes; off += chunk, slot ^= 1) {
+        const size_t len = std::min(chunk, bytes - off);
+        char* buf = stage_ring + size_t(slot) * kStageBytes;
+        if (stage_dev[slot] >= 0)   // the slot's last copy, from whichever device, is done
+            RB_CUDA_TRY(cudaEventSynchronize(stage_done[stage_dev[slot]][slot]));
+        const size_t units = len / unit, parts = size_t(pool.size());
+        pool.parallel([&](int k) {
+            const size_t a = units * size_t(k) / parts, b = units * size_t(k + 1) / parts;
+            if (b > a) fill(buf + a * unit, off + a * unit, (b - a) * unit);
+        });
+        RB_CUDA_TRY(cudaMemcpyAsync(dst + off, buf, len, cudaMemcpyHostToDevice, stream));
+        RB_CUDA_TRY(cudaEventRecord(stage_done[dev][slot], stream));
+        stage_dev[slot] = dev;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    const char* s = static_cast<const char*>(src);
+    return staged(static_cast<char*>(dst), bytes, 1, stream,
+                  [s](char* out, size_t first, size_t len) { std::memcpy(out, s + first, len); });
 }
 
 }  // namespace rb200

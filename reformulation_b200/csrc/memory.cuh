@@ -18,6 +18,14 @@ cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 void* pinned_get();          // a 256-byte pinned slot, or nullptr
 void pinned_put(void* slot);
 
+// Host-to-device copies of caller (pageable) memory through a library-owned
+// pinned staging ring: host threads fill one slot while the copy engine drains
+// the other, so the copy runs at the pinned rate instead of the driver's
+// pageable one.  Each call returns once its last chunk is queued on `stream`;
+// the caller's memory is no longer read after that.  Calls from several host
+// threads take turns.
+cudaError_t staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+
 template <class T>
 struct PoolBuf {
     T* ptr = nullptr;

@@ -1406,7 +1406,10 @@ struct Solver final : SolverBase {
         {
             PoolBuf<In> Hd;
             PoolBuf<double> part, tot;
-            RB_CUDA_TRY(Hd.upload(H, size_t(n) * t * t, stream));
+            // H (n t^2 values, the bulk of a solve's input) through the pinned
+            // staging ring
+            RB_CUDA_TRY(Hd.alloc(size_t(n) * t * t, stream));
+            RB_CUDA_TRY(staged_upload(Hd.ptr, H, sizeof(In) * size_t(n) * t * t, stream));
             RB_CUDA_TRY(part.alloc(kSquareBlocks, stream));
             RB_CUDA_TRY(tot.alloc(1, stream));
             h_squares_kernel<In><<<kSquareBlocks, 256, 0, stream>>>(n, t, Hd.ptr, part.ptr);

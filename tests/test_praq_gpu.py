@@ -148,6 +148,11 @@ def test_rejects_bad_input(lib):
     bad2 = QuboInstance("b", "b", 3, inst.diag, inst.rows.copy(), inst.cols.copy(), inst.vals)
     bad2.cols[0] = 3
     assert lib.solve(bad2, p).status == -2
+    # ends that wrap to valid int32 values must still be rejected
+    for v in (-1, (1 << 32) + 1, (1 << 31) + 2, -(1 << 32) + 2):
+        bad3 = QuboInstance("b", "b", 3, inst.diag, inst.rows.copy(), inst.cols.copy(), inst.vals)
+        bad3.rows[1] = v
+        assert lib.solve(bad3, p).status == -2
     empty = QuboInstance("e", "e", 0, np.zeros(0), np.zeros(0, np.int64), np.zeros(0, np.int64),
                          np.zeros(0))
     assert lib.solve(empty, p).status == -2
