@@ -803,6 +803,27 @@ z_kernel(Dev<Real> d, const Real* zsrc, int step, int gate) {
         z_task<Real, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
 }
 
+// The FP32 z kernel with registers capped for three CTAs per SM (two at its
+// natural 56): 2-3.5 % faster PRIA solves at T >= 500, neutral below; in FP64
+// the cap spills and was 2-4 % slower, so z_kernel<double> keeps its own.
+template <int kThreads, bool Reflect, bool Check, bool Pair>
+__global__ void __launch_bounds__(kThreads, 3)
+z_kernel_f32(Dev<float> d, const float* zsrc, int step, int gate) {
+    if constexpr (Pair)
+        z_task_pair<float, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
+    else
+        z_task<float, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
+}
+
+// the z kernel a precision launches
+template <class Real, int kThreads, bool Reflect, bool Check, bool Pair>
+constexpr auto z_entry() {
+    if constexpr (sizeof(Real) == 4)
+        return z_kernel_f32<kThreads, Reflect, Check, Pair>;
+    else
+        return z_kernel<Real, kThreads, Reflect, Check, Pair>;
+}
+
 // The primal bound terms at x for period block s (solver.py:347-365):
 // sum_i K_i max_{t>=s} x_ist, K0 max_{i, t>=s} x_ist and sum h x over the
 // block, restricted to t < tlimit and s < tlimit (tlimit = t for the unpadded
@@ -1520,7 +1541,7 @@ struct Solver final : SolverBase {
     cudaError_t yz_attr() {
         RB_CUDA_TRY(cudaFuncSetAttribute(y_kernel<Real, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(y_smem_limit())));
-        for (auto fn : {z_kernel<Real, kZThreads, R, C, false>, z_kernel<Real, kZThreads, R, C, true>}) {
+        for (auto fn : {z_entry<Real, kZThreads, R, C, false>(), z_entry<Real, kZThreads, R, C, true>()}) {
             RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
             RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         }
@@ -1573,8 +1594,8 @@ struct Solver final : SolverBase {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        if (d.zpair) return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C, true>, d, zs, step, gate);
-        return cudaLaunchKernelEx(&cfg, z_kernel<Real, kZThreads, R, C, false>, d, zs, step, gate);
+        if (d.zpair) return cudaLaunchKernelEx(&cfg, z_entry<Real, kZThreads, R, C, true>(), d, zs, step, gate);
+        return cudaLaunchKernelEx(&cfg, z_entry<Real, kZThreads, R, C, false>(), d, zs, step, gate);
     }
 
     cudaError_t launch_check(int mode) {
