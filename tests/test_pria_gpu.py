@@ -265,3 +265,22 @@ def test_z_block_pairs_equal_single_blocks(native, monkeypatch, precision, shape
     assert a.primal_objective == b.primal_objective and a.dual_objective == b.dual_objective
     for k in ("x", "y", "z"):
         assert np.array_equal(getattr(a, k), getattr(b, k))
+
+
+def test_concurrent_solves_from_host_threads(lib):
+    """pria_solve is thread-safe (the reference's contract, pria.h): solves
+    issued from several host threads at once, which share the library's
+    pinned upload ring and device pool, equal the same solves run one after
+    another, bit for bit."""
+    from concurrent.futures import ThreadPoolExecutor
+    insts = [jrp_demand(20 + k, 12 + 4 * k, 40 + 30 * k) for k in range(4)]
+    p = lib.parameters(-1, 1e-6)
+    alone = [lib.solve(j, p, precision=prec, want_solution=True)
+             for j, prec in zip(insts, ["fp64", "mixed", "fp64", "mixed"])]
+    with ThreadPoolExecutor(4) as ex:
+        together = list(ex.map(lambda a: lib.solve(a[0], p, precision=a[1], want_solution=True),
+                               zip(insts, ["fp64", "mixed", "fp64", "mixed"])))
+    for a, b in zip(alone, together):
+        assert a.iterations == b.iterations
+        assert a.primal_objective == b.primal_objective and a.dual_objective == b.dual_objective
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.z, b.z)
