@@ -284,3 +284,24 @@ def test_concurrent_solves_from_host_threads(lib):
         assert a.iterations == b.iterations
         assert a.primal_objective == b.primal_objective and a.dual_objective == b.dual_objective
         assert np.array_equal(a.x, b.x) and np.array_equal(a.z, b.z)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_zero_joint_and_item_costs_match_reference(lib, oracle_lib, precision):
+    """The corners of the reference's checks (jrp/pria-jax/tests/test_solver.py):
+    K0 = 0 (the z simplex is {0}: Michelot's threshold is +inf) and an item
+    with K_i = 0 (its y rows are {0}); bounds agree with ref::solve and the
+    returned point is feasible."""
+    base = jrp_demand(31, 6, 20)
+    k = base.order_costs.copy()
+    k[2] = 0.0
+    inst = JrpInstance("k0", "corner", k, 0.0, base.holding_costs)
+    ref = oracle_lib.ref_pria_solve(inst, oracle_lib.pria_params(tolerance=1e-6))
+    tol = 1e-6 if precision == "fp64" else 1e-4
+    s = lib.solve(inst, lib.parameters(-1, tol), precision=precision, want_solution=True)
+    assert s.status == 0 and s.relative_gap <= tol
+    assert rel(s.dual_objective, ref["lower"]) <= (1e-6 if precision == "fp64" else 1e-3)
+    assert rel(s.primal_objective, ref["upper"]) <= (1e-5 if precision == "fp64" else 1e-3)
+    assert np.all(s.z == 0) and np.all(s.y[2] == 0)
+    if precision == "fp64":
+        feasible(inst, s)
