@@ -301,3 +301,21 @@ def test_slot1_layouts_agree_sequential_gather(native, monkeypatch, use_float32)
     assert (a.status, a.iterations, a.lower, a.upper) == (b.status, b.iterations, b.lower, b.upper)
     assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
     assert a.lower <= a.upper
+
+
+@pytest.mark.parametrize("seed,n,density", [(0, 8, 0.5), (1, 10, 0.4), (2, 12, 0.3), (3, 12, 0.6)])
+def test_persistency_against_brute_force(lib, oracle_lib, seed, n, density):
+    """Weak persistency of the roof dual (qubo/praq-jax/tests/test_solver.py):
+    some binary minimiser of the QUBO, found by enumerating all 2^n points,
+    takes every value the relaxation optimum fixes."""
+    from reformulation_b200 import praq
+    inst = random_qubo(100 + seed, n, density)
+    s = lib.solve(inst, lib.parameters(tolerance=1e-10))
+    assert s.status == 0
+    fixed, vals = praq.persistent_variables(s.x)
+    points = ((np.arange(1 << n)[:, None] >> np.arange(n)) & 1).astype(np.float64)
+    values = np.array([oracle_lib.relaxation_value(inst, p) for p in points])
+    best = values.min()
+    assert s.lower <= best + 1e-9 * (1 + abs(best))     # the relaxation bounds the QUBO
+    optima = points[values <= best + 1e-9 * (1 + abs(best))]
+    assert np.any(np.all(optima[:, fixed] == vals[fixed], axis=1))
