@@ -68,7 +68,10 @@ constexpr int kLowTW = 32;              // columns per tile of the lower-bound p
 constexpr int kXTile = RB200_PRIA_XTILE;   // columns per tile of the x half-step (FP64 tile)
 constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
 constexpr int kMaxCluster = 16;
-constexpr int kUnroll = 4;           // rows per warp in flight (x kernel)
+// rows per warp in flight (x kernel): 6 in FP32, 4 in FP64 (measured best
+// of 2, 3, 4, 6, 8 for each; 6 in FP64 and 8 in either hold too many registers)
+template <class Real>
+constexpr int x_unroll() { return sizeof(Real) == 4 ? 6 : 4; }
 constexpr int kZUnroll = 8;          // z elements per thread in flight (z kernel)
 // y row values per lane in flight (y kernel): 8 in FP32, 4 in FP64 (more
 // registers per value; measured best of 4, 8, 16 for each)
@@ -256,6 +259,7 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
     const int tt = t0 + col;
     const double om = c->omega;
     const double tau = d.eta / om, sigma = d.eta * om;
+    constexpr int kUnroll = x_unroll<Real>();
     // rows are taken kUnroll at a time per warp so that their loads are in
     // flight together
     const int rstep = nwarps * kRpw;
