@@ -155,8 +155,12 @@ cudaError_t staged(char* dst, size_t bytes, size_t unit, cudaStream_t stream, Fi
     int dev = 0;
     RB_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!stage_ring) RB_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&stage_ring), 2 * kStageBytes,
-                                               cudaHostAllocPortable));
+    if (!stage_ring && cudaHostAlloc(reinterpret_cast<void**>(&stage_ring), 2 * kStageBytes,
+                                     cudaHostAllocPortable) != cudaSuccess) {
+        stage_ring = nullptr;
+        (void)cudaGetLastError();
+        return cudaErrorMemoryAllocation;   // the caller copies directly instead
+    }
     for (auto& ev : stage_done[dev])
         if (!ev) RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     HostThreads& pool = host_threads();
@@ -183,8 +187,11 @@ cudaError_t staged(char* dst, size_t bytes, size_t unit, cudaStream_t stream, Fi
 
 cudaError_t staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
     const char* s = static_cast<const char*>(src);
-    return staged(static_cast<char*>(dst), bytes, 1, stream,
-                  [s](char* out, size_t first, size_t len) { std::memcpy(out, s + first, len); });
+    const cudaError_t st = staged(static_cast<char*>(dst), bytes, 1, stream,
+                                  [s](char* out, size_t first, size_t len) { std::memcpy(out, s + first, len); });
+    // no pinned ring to be had: the driver's own (pageable) copy
+    if (st == cudaErrorMemoryAllocation) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+    return st;
 }
 
 }  // namespace rb200
