@@ -79,11 +79,12 @@ def build_cli(force: bool = False) -> list[Path]:
     out = []
     cxx = shutil.which("g++") or "g++"
     for src, exe in cli_targets():
-        deps = [src, LIB] + sorted((ROOT / "include").glob("*.h"))
+        deps = [src, LIB] + sorted((ROOT / "include").glob("*.h")) + sorted(CLI_SRC.glob("*.hpp"))
         if not force and exe.exists() and all(d.stat().st_mtime <= exe.stat().st_mtime for d in deps):
             out.append(exe)
             continue
-        cmd = [cxx, "-O2", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", f"-I{CUDA_HOME / 'include'}",
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-Wextra", f"-I{ROOT / 'include'}", f"-I{CLI_SRC}",
+               f"-I{CUDA_HOME / 'include'}",
                str(src), "-o", str(exe), f"-L{OUT}", "-lreform_b200", f"-L{CUDA_HOME / 'lib64'}", "-lcudart",
                "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME / 'lib64'}"]
         res = subprocess.run(cmd, capture_output=True, text=True)

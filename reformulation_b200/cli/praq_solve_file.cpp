@@ -1,135 +1,92 @@
-// praq_solve_file -- the file-driven PRAQ solve, over this library's C ABI.
+// praq_solve_file -- the QUBO roof-dual LP solver as a file-in, file-out
+// program, for harnesses that run a solver as a subprocess
+// (qubo/harness/backends/praq_cuda.py:79-167 drives it this way).
 //
-// Drop-in for the reference's CLI (qubo/praq-cuda/tools/praq_solve_file.cu:1-31),
-// which its harness backend (qubo/harness/backends/praq_cuda.py:27-86) runs as
-// a subprocess.  The wire formats and the exit codes are that contract, so they
-// are the same here; the program itself is this project's.
+//   praq_solve_file <instance> <result> [tol] [max_iter] [f32]
 //
-//   instance (little-endian):  i64 magic 0x51415250, i64 n, i64 m,
-//                              f64 diag[n], i64 rows[m], i64 cols[m], f64 vals[m]
-//   result:                    i64 n, i64 iterations, i64 status,
-//                              f64 lower, f64 upper, f64 x[n]
+//   tol       relative duality gap to stop at (default: the library's)
+//   max_iter  iteration cap; 0 or absent keeps the library's default
+//   f32       FP32 iterates with FP64 reductions and bounds
 //
-//   usage: praq_solve_file <instance> <result> [tol] [max_iter] [f32]
-//   exit:  0 converged, 1 iteration limit, 2 usage / unreadable input /
-//          unwritable result, 3 the solver failed (no result file is written)
-//
-// Stdout repeats the result as "key: value" lines, with setup_seconds (file
-// read + CUDA context) and solve_seconds (the praq_solve call), which the
-// harness parses (praq_cuda.py:_timings).
-#include <chrono>
-#include <cstdint>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <vector>
-
-#include <cuda_runtime_api.h>
+// The file formats, exit codes and the two timing keys are those of
+// wire_format.hpp.  The solve goes through praq_solve, the reference-facing
+// entry point of include/praq.h.
+#include <cuda_runtime.h>
 
 #include "praq.h"
+#include "wire_format.hpp"
 
 namespace {
 
-constexpr int64_t kMagic = 0x51415250;   // "PRAQ"
+constexpr const char* kTool = "praq_solve_file";
+constexpr const char* kUsage =
+    "usage: praq_solve_file <instance> <result> [tol] [max_iter] [f32]";
 
-using Clock = std::chrono::steady_clock;
-
-double since(Clock::time_point t0) {
-    return std::chrono::duration<double>(Clock::now() - t0).count();
+const char* status_name(int status) {
+    switch (status) {
+        case 0: return "converged";
+        case 1: return "iteration_limit";
+        default: return "error";
+    }
 }
-
-// Reads `count` items of T; false on a short file.
-template <class T>
-bool read_items(FILE* f, std::vector<T>& v, int64_t count) {
-    if (count < 0) return false;
-    v.resize(size_t(count));
-    return count == 0 || std::fread(v.data(), sizeof(T), size_t(count), f) == size_t(count);
-}
-
-struct FileCloser {
-    FILE* f;
-    ~FileCloser() { if (f) std::fclose(f); }
-};
 
 }  // namespace
 
 int main(int argc, char** argv) {
-    if (argc < 3 || argc > 6) {
-        std::fprintf(stderr, "usage: %s <instance> <result> [tol] [max_iter] [f32]\n", argv[0]);
-        return 2;
-    }
+    namespace w = rb200::wire;
+    const w::Stopwatch setup_clock;
+
+    w::Invocation args;
+    if (std::string why = w::parse(argc, argv, {"f32"}, args); !why.empty())
+        return w::fail(w::kBadInput, kTool, why + "\n" + kUsage);
+
+    w::QuboFile qubo;
+    if (std::string why = w::load(args.instance, qubo); !why.empty())
+        return w::fail(w::kBadInput, kTool, args.instance + ": " + why);
+
     PraqParameters params = praq_default_parameters();
-    if (argc > 3) params.tolerance = std::atof(argv[3]);
-    if (argc > 4) params.max_iter = std::atoll(argv[4]);
-    if (argc > 5) params.use_float32 = std::strcmp(argv[5], "f32") == 0 ? 1 : 0;
+    if (args.has_tolerance) params.tolerance = args.tolerance;
+    if (args.has_max_iter && args.max_iter != 0) params.max_iter = args.max_iter;
+    params.use_float32 = args.flag("f32") ? 1 : 0;
 
-    const auto t_setup = Clock::now();
-    std::vector<double> diag, vals;
-    std::vector<int64_t> rows, cols;
-    int64_t head[3] = {0, 0, 0};
-    {
-        FileCloser in{std::fopen(argv[1], "rb")};
-        if (!in.f) {
-            std::fprintf(stderr, "praq_solve_file: cannot open %s\n", argv[1]);
-            return 2;
-        }
-        const bool ok = std::fread(head, sizeof(int64_t), 3, in.f) == 3 && head[0] == kMagic &&
-                        head[1] >= 0 && head[2] >= 0 && read_items(in.f, diag, head[1]) &&
-                        read_items(in.f, rows, head[2]) && read_items(in.f, cols, head[2]) &&
-                        read_items(in.f, vals, head[2]);
-        if (!ok) {
-            std::fprintf(stderr, "praq_solve_file: %s is not a PRAQ instance file\n", argv[1]);
-            return 2;
-        }
-    }
-    PraqInstance inst;
-    inst.n = head[1];
-    inst.m = head[2];
-    inst.diag = diag.data();
-    inst.rows = rows.data();
-    inst.cols = cols.data();
-    inst.vals = vals.data();
+    // The CUDA context belongs to set-up, not to the solve.
+    if (cudaInitDevice(0, 0, 0) != cudaSuccess || cudaSetDevice(0) != cudaSuccess)
+        return w::fail(w::kSolverFailed, kTool, "no usable CUDA device");
+    const double setup_seconds = setup_clock.seconds();
 
-    cudaFree(nullptr);   // context creation belongs to set-up, not to the solve
-    const double setup_seconds = since(t_setup);
+    const PraqInstance view{qubo.n, qubo.m, qubo.diag.data(), qubo.rows.data(), qubo.cols.data(),
+                            qubo.vals.data()};
+    std::vector<double> x(size_t(qubo.n));
+    PraqResult result{};
+    const w::Stopwatch solve_clock;
+    const int status = praq_solve(&view, &params, x.data(), &result);
+    const double solve_seconds = solve_clock.seconds();
+    if (status < 0)
+        return w::fail(w::kSolverFailed, kTool,
+                       "praq_solve returned error " + std::to_string(status));
 
-    std::vector<double> x(size_t(inst.n));
-    PraqResult res;
-    const auto t_solve = Clock::now();
-    const int rc = praq_solve(&inst, &params, x.data(), &res);
-    const double solve_seconds = since(t_solve);
-    if (rc < 0) {
-        std::fprintf(stderr, "praq_solve_file: praq_solve failed with status %d\n", rc);
-        return 3;
-    }
+    w::Record record;
+    record.word(qubo.n).word(result.iterations).word(status);
+    record.real(result.lower).real(result.upper);
+    record.array(x.data(), x.size());
+    if (std::string why = record.commit(args.result); !why.empty())
+        return w::fail(w::kSolverFailed, kTool, why);
 
-    {
-        FileCloser out{std::fopen(argv[2], "wb")};
-        if (!out.f) {
-            std::fprintf(stderr, "praq_solve_file: cannot write %s\n", argv[2]);
-            return 2;
-        }
-        const int64_t words[3] = {inst.n, res.iterations, int64_t(res.status)};
-        const double bounds[2] = {res.lower, res.upper};
-        bool ok = std::fwrite(words, sizeof(int64_t), 3, out.f) == 3 &&
-                  std::fwrite(bounds, sizeof(double), 2, out.f) == 2 &&
-                  std::fwrite(x.data(), sizeof(double), x.size(), out.f) == x.size();
-        ok = std::fclose(out.f) == 0 && ok;
-        out.f = nullptr;
-        if (!ok) {
-            std::fprintf(stderr, "praq_solve_file: short write to %s\n", argv[2]);
-            return 2;
-        }
-    }
-
-    std::printf("n: %lld\n", (long long)inst.n);
-    std::printf("edges: %lld\n", (long long)inst.m);
-    std::printf("precision: %s\n", params.use_float32 ? "float32" : "float64");
-    std::printf("status: %s\n", res.status == 0 ? "converged" : "iteration_limit");
-    std::printf("iterations: %lld\n", (long long)res.iterations);
-    std::printf("lower: %.17g\n", res.lower);
-    std::printf("upper: %.17g\n", res.upper);
-    std::printf("setup_seconds: %.6f\n", setup_seconds);
-    std::printf("solve_seconds: %.6f\n", solve_seconds);
-    return res.status == 0 ? 0 : 1;
+    const double gap =
+        (result.upper - result.lower) / (1.0 + std::fabs(result.upper) + std::fabs(result.lower));
+    w::Report()
+        .add("instance", args.instance)
+        .add("nodes", qubo.n)
+        .add("edges", qubo.m)
+        .add("precision", std::string(params.use_float32 ? "float32" : "float64"))
+        .add("tolerance", params.tolerance)
+        .add("status", std::string(status_name(status)))
+        .add("iterations", result.iterations)
+        .add("lower", result.lower)
+        .add("upper", result.upper)
+        .add("relative_gap", gap)
+        .add("setup_seconds", setup_seconds)
+        .add("solve_seconds", solve_seconds)
+        .print();
+    return status == 0 ? w::kConverged : w::kIterationLimit;
 }
