@@ -108,7 +108,9 @@ def test_batch_admission_while_running_and_removal(native, oracle_lib):
         b.remove(first[1])
         assert b.device_bytes() < before
         flow = oracle_lib.roof_dual_maxflow(qs[0])
-        assert rel(b.result_qubo(first[0]).upper, flow) <= 1e-3
+        r0 = b.result_qubo(first[0])
+        assert r0.lower <= flow + 1e-7 * (1 + abs(flow)) <= r0.upper + 2e-7 * (1 + abs(flow))
+        assert r0.gap <= 1e-4
 
 
 def test_autotune_keeps_results(native):
@@ -125,7 +127,7 @@ def test_autotune_keeps_results(native):
         b.run()
         for i in range(2):
             r = b.result_qubo(i)
-            assert rel(r.upper, sq[i].upper) <= 1e-3 and r.status == 0
+            assert rel(r.upper, sq[i].upper) <= 1e-6 and r.status == 0
         for i in range(2):
             r = b.result_jrp(2 + i)
             assert r.iterations == sj[i].iterations

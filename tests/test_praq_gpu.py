@@ -11,8 +11,8 @@ restatement (iterations and bounds) and with the max-flow roof dual.
 Tolerances: FP64 bounds agree with the optimum to 1e-7 relative at a 1e-9 gap;
 FP64 iteration counts agree with the oracle's exactly on these instances (same
 arithmetic, different summation order can move a check by one block, so
-+-op_steps is allowed); FP32 ("mixed") results agree to 1e-3 relative at a 1e-4
-gap.
++-op_steps is allowed); FP32 ("mixed") objectives agree with the FP64
+oracle's to 1e-6 relative at the same 1e-4 gap tolerance.
 """
 
 import numpy as np
@@ -82,11 +82,15 @@ def test_bounds_bracket_under_every_cap(lib, oracle_lib):
 
 @pytest.mark.parametrize("n", [4, 6, 8])
 def test_float32_accuracy(lib, oracle_lib, n):
+    """FP32 iterates: the objective within 1e-6 relative of the FP64 oracle's
+    at the same 1e-4 gap tolerance, and a bracket of the optimum."""
     inst = random_qubo(200 + n, n, 0.7)
     opt = oracle_lib.half_integral_optimum(inst)
+    ref = oracle_lib.praq_solve(inst, oracle_lib.praq_params(tolerance=1e-4))
     s = lib.solve(inst, lib.parameters(tolerance=1e-4, use_float32=1))
-    assert s.status == 0
-    assert rel(s.upper, opt) <= 1e-3 and rel(s.lower, opt) <= 1e-3
+    assert s.status == 0 and s.gap <= 1e-4
+    assert rel(s.upper, ref["upper"]) <= 1e-6
+    assert s.lower <= opt + 1e-7 * (1 + abs(opt)) and s.upper >= opt - 1e-7 * (1 + abs(opt))
 
 
 def test_larger_instance_certifies_itself(lib, oracle_lib):
@@ -179,8 +183,9 @@ def test_backend_solve_api(native):
     assert r.iterations > 0 and np.isnan(r.feasibility_tolerance)
     m = praq.solve(inst, tolerances=Tolerances(optimality=1e-4), time_limit=60.0,
                    precision="mixed")
-    assert m.status == "optimal"
-    assert rel(m.objective, r.objective) <= 1e-3
+    f = praq.solve(inst, tolerances=Tolerances(optimality=1e-4), time_limit=60.0)
+    assert m.status == "optimal" and f.status == "optimal"
+    assert rel(m.objective, f.objective) <= 1e-6
     c = praq.solve(inst, tolerances=Tolerances(optimality=1e-12), time_limit=60.0, max_iter=32)
     assert c.status == "iteration_limit" and np.isnan(c.objective) and c.lower <= c.upper
 
@@ -319,3 +324,49 @@ def test_persistency_against_brute_force(lib, oracle_lib, seed, n, density):
     assert s.lower <= best + 1e-9 * (1 + abs(best))     # the relaxation bounds the QUBO
     optima = points[values <= best + 1e-9 * (1 + abs(best))]
     assert np.any(np.all(optima[:, fixed] == vals[fixed], axis=1))
+
+
+def test_time_limit_stops_with_a_valid_bracket(native, oracle_lib):
+    """reform_praq_set_time_limit: a run past its budget stops between checks
+    with PRAQ_STATUS_TIME_LIMIT and the bracket of the last completed check
+    (both iterates are feasible, so it brackets the optimum); the backend
+    reports status "time_limit" with those bounds."""
+    from reformulation_b200 import praq
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.results import Tolerances
+    inst = qubo_uniform_edges(6, 20_000, 100_000)
+    flow = oracle_lib.roof_dual_maxflow(inst)
+    p = praq.Library().parameters(tolerance=1e-12)
+    with praq.DeviceSolver(inst, p) as dev:
+        dev.set_time_limit(0.0)
+        assert dev.run() == 2
+        r = dev.result()
+        assert r.status == 2 and 0 < r.iterations <= 64
+        assert r.lower <= flow + 1e-9 * (1 + abs(flow)) <= r.upper + 2e-9 * (1 + abs(flow))
+    res = praq.solve(inst, tolerances=Tolerances(optimality=1e-12), time_limit=0.0)
+    assert res.status == "time_limit" and res.lower <= res.upper and np.isnan(res.objective)
+
+
+def test_beyond_two_to_the_26_nodes(native, oracle_lib):
+    """praq_solve takes the reference's sizes, n up to INT_MAX
+    (qubo/praq-cuda/src/solver.cuh:525-526): n = 70,000,000 nodes (above
+    2^26) and 300,000 uniform edges.  The optimum is the max-flow roof dual of
+    the nodes the edges touch plus sum min(d_i, 0) over the others (an
+    isolated node takes x_i = 1 exactly when d_i < 0)."""
+    from reformulation_b200.instances import qubo_uniform_edges
+    inst = qubo_uniform_edges(9, 70_000_000, 300_000)
+    touched = np.unique(np.concatenate([inst.rows, inst.cols]))
+    alone = np.ones(inst.n, bool)
+    alone[touched] = False
+    remap = np.full(inst.n, -1, np.int64)
+    remap[touched] = np.arange(touched.size)
+    sub = QuboInstance("sub", "sub", touched.size, inst.diag[touched], remap[inst.rows],
+                       remap[inst.cols], inst.vals)
+    opt = np.minimum(inst.diag[alone], 0.0).sum() + oracle_lib.roof_dual_maxflow(sub)
+    from reformulation_b200.praq import Library
+    lib = Library()
+    s = lib.solve(inst, lib.parameters(tolerance=1e-7))
+    assert s.status == 0 and s.gap <= 1e-7
+    assert s.lower <= opt + 1e-9 * abs(opt) and s.upper >= opt - 1e-9 * abs(opt)
+    assert rel(s.upper, opt) <= 1e-6
+    assert np.all((s.x >= 0) & (s.x <= 1))
