@@ -158,9 +158,17 @@ REFORM_API void reform_praq_destroy(reform_praq_solver* solver);
  * device current) and caches it: make that first call before any stream
  * capture.  Calls share the array, so calls whose work overlaps on the GPU
  * (two streams, or two threads) race and give wrong results; serialise them.
- * An out-of-range edge index is skipped and both outputs become NaN.
+ * The cached address does not survive cudaDeviceReset (the reset unloads the
+ * array): after a reset, do not call this entry point again in the process.
+ * Edge indices are checked on the device, not the host: an edge with an index
+ * out of range or with i == j (a self-loop, which the instance format does not
+ * allow) is skipped and both outputs become NaN.  The per-node sums of S^T y
+ * use FP64 atomic additions, so the lower bound is not bitwise reproducible:
+ * its last bits can differ from call to call (the upper bound's do not).
  * Returns 0, PRAQ_ERROR_ARGUMENT for a null pointer, PRAQ_ERROR_INSTANCE for
- * n or m out of range, PRAQ_ERROR_CUDA if the launch failed. */
+ * n or m out of range, PRAQ_ERROR_CUDA if a launch failed or if a CUDA error
+ * was already pending on the calling thread (it is left pending, and nothing
+ * is launched). */
 REFORM_API int reform_praq_bounds_noalloc(int64_t n, int64_t m, const double* diag,
                                           const int64_t* rows, const int64_t* cols,
                                           const double* vals, const double* x,

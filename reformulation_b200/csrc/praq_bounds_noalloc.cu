@@ -30,7 +30,8 @@ namespace noalloc {
 //   [kMaxNodes, kMaxNodes + 4 kBlocks)   two partial rows (upper, lower) per
 //                                        block, for the edge pass then the
 //                                        node pass
-//   [kMaxNodes + 4 kBlocks]              a flag: an index was out of range
+//   [kMaxNodes + 4 kBlocks]              a flag: an edge index was out of
+//                                        range, or an edge was a self-loop
 constexpr long long kMaxNodes = 1LL << 18;   // 262,144 nodes: 2 MiB of doubles
 constexpr int kBlocks = 296;                 // fixed grid: 2 blocks per SM on 148 SMs
 constexpr int kThreads = 256;
@@ -45,8 +46,10 @@ __global__ void clear_kernel(long long n, double* __restrict__ s) {
     if (blockIdx.x == 0 && threadIdx.x == 0) s[kMaxNodes + 4 * kBlocks] = 0.0;
 }
 
-// Edge pass: accumulate both half-edge duals into S^T y (atomics), and the
-// edge parts of both bounds into this block's partial row.
+// Edge pass: accumulate both half-edge duals into S^T y (FP64 atomics, so
+// the order of the additions into one node, and with it the last bits of the
+// lower bound, can change from call to call), and the edge parts of both
+// bounds into this block's partial row.
 __global__ void __launch_bounds__(kThreads)
 edge_pass(long long n, long long m, const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
           const double* __restrict__ vals, const double* __restrict__ x, const double* __restrict__ y,
@@ -57,7 +60,7 @@ edge_pass(long long n, long long m, const int64_t* __restrict__ rows, const int6
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) {
         const int64_t i = rows[e], j = cols[e];
-        if (i < 0 || i >= n || j < 0 || j >= n) {
+        if (i < 0 || i >= n || j < 0 || j >= n || i == j) {   // out of range or a self-loop
             bad = true;
             continue;
         }
@@ -96,7 +99,7 @@ node_pass(long long n, const double* __restrict__ diag, const double* __restrict
 }
 
 // One block: both sets of partial rows, in a fixed order, into out[0] (lower)
-// and out[1] (upper); NaN for both if an edge index was out of range.
+// and out[1] (upper); NaN for both if an edge was out of range or a self-loop.
 __global__ void __launch_bounds__(kThreads) finish(const double* __restrict__ s, double* __restrict__ out) {
     __shared__ double scratch[2 * 32];
     __shared__ double total[2];
@@ -109,7 +112,8 @@ __global__ void __launch_bounds__(kThreads) finish(const double* __restrict__ s,
 }
 
 // The device address of g_scratch, looked up once per device (with that
-// device current) and cached.
+// device current) and cached for the life of the process: a cudaDeviceReset
+// unloads the module and leaves the cached address stale.
 static double* scratch_address() {
     static std::mutex mu;
     static double* cache[64] = {};
@@ -134,12 +138,19 @@ extern "C" int reform_praq_bounds_noalloc(int64_t n, int64_t m, const double* di
     using namespace rb200::noalloc;
     if (!diag || !x || !out || (m > 0 && (!rows || !cols || !vals || !y))) return PRAQ_ERROR_ARGUMENT;
     if (n <= 0 || n > kMaxNodes || m < 0) return PRAQ_ERROR_INSTANCE;
+    // An error the caller left pending on this thread is reported, not
+    // cleared, and nothing is launched; after that check every error of the
+    // launches below is this call's own.
+    if (cudaPeekAtLastError() != cudaSuccess) return PRAQ_ERROR_CUDA;
     double* s = scratch_address();
     if (!s) return PRAQ_ERROR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     clear_kernel<<<kBlocks, kThreads, 0, st>>>(n, s);
+    if (cudaGetLastError() != cudaSuccess) return PRAQ_ERROR_CUDA;
     edge_pass<<<kBlocks, kThreads, 0, st>>>(n, m, rows, cols, vals, x, y, s);
+    if (cudaGetLastError() != cudaSuccess) return PRAQ_ERROR_CUDA;
     node_pass<<<kBlocks, kThreads, 0, st>>>(n, diag, x, s);
+    if (cudaGetLastError() != cudaSuccess) return PRAQ_ERROR_CUDA;
     finish<<<1, kThreads, 0, st>>>(s, out);
     return cudaGetLastError() == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
 }

@@ -72,3 +72,83 @@ def test_noalloc_rejects_beyond_its_scratch(native):
     assert L.reform_praq_bounds_noalloc(262_145, 0, p, None, None, None, p, None, p, None) == -2
     assert L.reform_praq_bounds_noalloc(0, 0, p, None, None, None, p, None, p, None) == -2
     assert L.reform_praq_bounds_noalloc(4, 0, None, None, None, None, p, None, p, None) == -1
+
+
+def _bracket(inst, x, y):
+    """The entry point on device copies of (instance, x, y): (rc, lower, upper)."""
+    import torch
+
+    from reformulation_b200 import _native
+    args = [_device(a) for a in (np.asarray(inst.diag, np.float64), np.asarray(inst.rows, np.int64),
+                                 np.asarray(inst.cols, np.int64), np.asarray(inst.vals, np.float64),
+                                 np.asarray(x, np.float64), np.asarray(y, np.float64).reshape(-1))]
+    if inst.edges == 0:      # an empty tensor may have no address: pass a valid one
+        args[1] = args[2] = _device(np.zeros(1, np.int64))
+        args[3] = args[5] = _device(np.zeros(2))
+    out = torch.full((2,), 7.0, dtype=torch.float64, device="cuda")
+    rc = _native.lib().reform_praq_bounds_noalloc(inst.n, inst.edges, *[a.data_ptr() for a in args],
+                                                  out.data_ptr(),
+                                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    lower, upper = out.tolist()
+    return rc, lower, upper
+
+
+def test_noalloc_bad_edges_give_nan(native):
+    """An edge index out of range, or a self-loop, is flagged on the device:
+    both outputs are NaN; the next valid call is unaffected."""
+    from reformulation_b200.instances import QuboInstance
+    rng = np.random.default_rng(2)
+    n = 50
+    rows, cols = rng.integers(0, n, 40), rng.integers(0, n, 40)
+    rows, cols = np.minimum(rows, cols), np.maximum(rows, cols)
+    keep = rows != cols
+    base = QuboInstance("b", "b", n, rng.normal(size=n), rows[keep], cols[keep],
+                        rng.normal(size=keep.sum()))
+    x, y = rng.uniform(0, 1, n), rng.normal(size=(base.edges, 2))
+    for bad_col in (n, -1, int(base.rows[3])):      # past the end, negative, a self-loop
+        c = base.cols.copy()
+        c[3] = bad_col
+        bad = QuboInstance("x", "x", n, base.diag, base.rows, c, base.vals)
+        rc, lower, upper = _bracket(bad, x, y)
+        assert rc == 0 and np.isnan(lower) and np.isnan(upper), bad_col
+    rc, lower, upper = _bracket(base, x, y)
+    assert rc == 0 and np.isfinite(lower) and np.isfinite(upper)
+
+
+def test_noalloc_without_edges(native):
+    """m = 0: the node pass alone, lower = sum min(d, 0) and upper = d.x."""
+    from reformulation_b200.instances import QuboInstance
+    rng = np.random.default_rng(3)
+    n = 1000
+    inst = QuboInstance("e", "e", n, rng.normal(size=n), np.zeros(0, np.int64), np.zeros(0, np.int64),
+                        np.zeros(0))
+    x = rng.uniform(0, 1, n)
+    rc, lower, upper = _bracket(inst, x, np.zeros(0))
+    assert rc == 0
+    assert rel(lower, np.minimum(inst.diag, 0).sum()) <= 1e-12
+    assert rel(upper, inst.diag @ x) <= 1e-12
+
+
+def test_noalloc_at_its_largest_instance(native, oracle_lib):
+    """n = 262,144, the largest instance the fixed scratch holds (the last
+    node's accumulator is its last S^T y slot), against the oracle's bracket
+    of the same point."""
+    from reformulation_b200.instances import qubo_uniform_edges
+    n = 262_144
+    inst = qubo_uniform_edges(8, n, 40_000)
+    rng = np.random.default_rng(4)
+    x = rng.uniform(0, 1, n)
+    w = 2.0 * np.abs(inst.vals)
+    y = np.where((inst.vals > 0)[:, None], -0.5 * w[:, None], 0.5 * w[:, None]) * np.ones((1, 2))
+    # an edge at the very last node, so the scratch boundary is exercised
+    rows = np.append(inst.rows, 0)
+    cols = np.append(inst.cols, n - 1)
+    vals = np.append(inst.vals, -3.0)
+    y = np.vstack([y, [3.0, 3.0]])
+    from reformulation_b200.instances import QuboInstance
+    full = QuboInstance("big", "big", n, inst.diag, rows, cols, vals)
+    rc, lower, upper = _bracket(full, x, y)
+    assert rc == 0
+    assert rel(upper, oracle_lib.relaxation_value(full, x)) <= 1e-12
+    assert rel(lower, oracle_lib.qubo_lower_bound(full, y)) <= 1e-12
