@@ -108,8 +108,20 @@ REFORM_API int reform_pria_create(int64_t n, int64_t t, const double* order_cost
                                   reform_pria_solver** out);
 
 /* One full solve from the cold start (or from the warm start last given with
- * reform_pria_set_warm).  Blocks the host until done.  Returns 0 or an error. */
+ * reform_pria_set_warm).  Blocks the host until done.  Returns 0, a CUDA
+ * error code, or REFORM_PRIA_STATUS_TIME_LIMIT (below). */
 REFORM_API int reform_pria_run(reform_pria_solver* solver);
+
+/* A wall-clock budget for each run, in seconds (< 0: none, the default); no
+ * counterpart in the reference's library, whose harness kills the solver
+ * process past the limit (jrp/harness/backends/pria_cuda.py:114-145).  The
+ * host checks it each time a convergence check's result arrives; when it has
+ * run out, the run stops there (the block already in flight finishes) and
+ * returns REFORM_PRIA_STATUS_TIME_LIMIT, and reform_pria_result gives the point
+ * and the bracket of the last completed check -- a valid bracket, since every
+ * iterate is feasible.  A run that converges in the same block returns 0. */
+#define REFORM_PRIA_STATUS_TIME_LIMIT (-1)
+REFORM_API int reform_pria_set_time_limit(reform_pria_solver* solver, double seconds);
 
 /* Warm start for the next runs: dense [n][t][t] FP64 arrays in the output
  * convention (duals normalised); NULL pointers clear it. */

@@ -97,6 +97,7 @@ def _declare(lib):
         "reform_pria_create": (I, [c_int64, c_int64, D, c_double, D, P(PriaParams), I, c_void_p,
                                    P(c_void_p)]),
         "reform_pria_run": (I, [c_void_p]),
+        "reform_pria_set_time_limit": (I, [c_void_p, c_double]),
         "reform_pria_set_warm": (I, [c_void_p, D, D, D]),
         "reform_pria_result": (I, [c_void_p, D, D, D, P(PriaResultInfo)]),
         "reform_pria_run_profiled": (I, [c_void_p, D, P(c_int64)]),

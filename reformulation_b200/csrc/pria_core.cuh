@@ -1059,10 +1059,12 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* _
         c->terminated = 1;
         c->result_slot = 2;
         c->restart = 0;
-    } else if (restart) {
-        c->restart = 1;
     } else {
-        c->check_error = new_err;
+        // the gap was measured at the step (x2s, y2s, z2s); a restart step
+        // that follows makes that point the anchor and sets result_slot = 1
+        c->result_slot = 2;
+        if (restart) c->restart = 1;
+        else c->check_error = new_err;
     }
 }
 
@@ -1306,7 +1308,13 @@ __global__ void sum_rows_kernel(const double* __restrict__ partial, int count, d
 // ---------------------------------------------------------------------------
 // host side
 
+// reform_pria_run's return value when the wall-clock budget ran out.
+constexpr int kStatusTimeLimit = REFORM_PRIA_STATUS_TIME_LIMIT;
+
 struct SolverBase {
+    // Wall-clock budget of each run, in seconds; < 0: none.  Checked on the
+    // host each time a check's result arrives.
+    double time_limit = -1.0;
     virtual ~SolverBase() = default;
     virtual int run() = 0;
     virtual int result(double* x, double* y, double* z, pria_result_info* info) = 0;
@@ -1725,7 +1733,13 @@ struct Solver final : SolverBase {
     // The vanilla phase from the start point (x0, the anchor, is kept for
     // the drift that sets omega), then, for the Halpern method, the step
     // that makes the current point the anchor (mode 4).
-    cudaError_t run_vanilla() {
+    // Seconds since `started`, against the budget.
+    bool over_budget(std::chrono::steady_clock::time_point started) const {
+        return time_limit >= 0.0 &&
+               std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() > time_limit;
+    }
+
+    cudaError_t run_vanilla(std::chrono::steady_clock::time_point started, bool& timed_out) {
         const size_t bytes = sizeof(Real) * size_t(nd);
         RB_CUDA_TRY(cudaMemcpyAsync(d.xh, d.x0, bytes, cudaMemcpyDeviceToDevice, stream));
         RB_CUDA_TRY(cudaMemcpyAsync(d.yh, d.y0, bytes, cudaMemcpyDeviceToDevice, stream));
@@ -1734,6 +1748,10 @@ struct Solver final : SolverBase {
             RB_CUDA_TRY(enqueue_vanilla_block());
             RB_CUDA_TRY(cudaStreamSynchronize(stream));
             if (mirror->terminated || mirror->phase_done) break;
+            if (over_budget(started)) {
+                timed_out = true;        // the last check's point: the current one (slot 3)
+                return cudaSuccess;
+            }
             if (p.verbose)
                 fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  (vanilla)\n",
                         mirror->iteration, mirror->upper, mirror->lower, mirror->gap);
@@ -1748,10 +1766,14 @@ struct Solver final : SolverBase {
     }
 
     int run() override {
+        const auto started = std::chrono::steady_clock::now();
+        bool timed_out = false;
         if (runs++ > 0 && !exec && p.use_halpern && capture_block() != cudaSuccess) return int(cudaErrorUnknown);
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
-        if (!mirror->terminated && vanilla_phase() && (st = run_vanilla()) != cudaSuccess) return int(st);
+        if (!mirror->terminated && vanilla_phase() && (st = run_vanilla(started, timed_out)) != cudaSuccess)
+            return int(st);
+        if (timed_out && !mirror->terminated) return kStatusTimeLimit;
         if (!mirror->terminated) {
             for (int kk = 0; kk < 2; ++kk) {
                 if ((st = launch_block()) != cudaSuccess) return int(st);
@@ -1765,16 +1787,23 @@ struct Solver final : SolverBase {
                 if (p.verbose)
                     fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  omega %.3e\n",
                             mirror->iteration, mirror->upper, mirror->lower, mirror->gap, mirror->omega);
+                if (over_budget(started)) {
+                    timed_out = true;
+                    break;
+                }
                 if ((st = launch_block()) != cudaSuccess) return int(st);
                 if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
                 nlaunch += block_nodes;
                 kk ^= 1;
             }
         }
+        // The block still in flight after a time-out finishes (its check
+        // included) before the mirror is read back; the result is the point and
+        // bracket of the last check it completed.
         if ((st = cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
             (st = cudaStreamSynchronize(stream)) != cudaSuccess)
             return int(st);
-        return 0;
+        return timed_out && !mirror->terminated ? kStatusTimeLimit : 0;
     }
 
     int run_profiled(double* ms, long long* count) override {
@@ -1782,7 +1811,13 @@ struct Solver final : SolverBase {
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
         // the vanilla phase, if any, runs untimed: the kinds are the Halpern block's
-        if (!mirror->terminated && vanilla_phase() && (st = run_vanilla()) != cudaSuccess) return int(st);
+        bool timed_out = false;   // no budget here: time_limit is not consulted by a profiled run
+        const auto never = std::chrono::steady_clock::now();
+        const double budget = time_limit;
+        time_limit = -1.0;
+        st = !mirror->terminated && vanilla_phase() ? run_vanilla(never, timed_out) : cudaSuccess;
+        time_limit = budget;
+        if (st != cudaSuccess) return int(st);
         profiling = true;
         while (!mirror->terminated) {
             marks.clear();

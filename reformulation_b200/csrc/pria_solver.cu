@@ -137,6 +137,12 @@ int reform_pria_run(reform_pria_solver* solver) {
     return solver->impl->run();
 }
 
+int reform_pria_set_time_limit(reform_pria_solver* solver, double seconds) {
+    if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
+    solver->impl->time_limit = seconds;
+    return 0;
+}
+
 int reform_pria_set_warm(reform_pria_solver* solver, const double* wx, const double* wy, const double* wz) {
     if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
     return solver->impl->set_warm(wx, wy, wz);

@@ -27,6 +27,10 @@ SCHEDULE = ("omega", "beta_sufficient", "beta_artificial", "beta_necessary", "th
             "theta_target", "theta_decay", "op_steps")
 
 
+#: reform_pria_run's status when the wall-clock budget ran out (include/pria.h).
+TIME_LIMIT = -1
+
+
 @dataclass(frozen=True)
 class Solve:
     """One solve: status (0 or a CUDA error code), bounds, iterations, solution."""
@@ -112,6 +116,13 @@ class DeviceSolver:
             raise RuntimeError(f"reform_pria_create failed with status {st}")
         self._h = handle
 
+    def set_time_limit(self, seconds: float) -> None:
+        """Wall-clock budget of each later run (seconds; < 0: none).  A run that
+        exceeds it returns TIME_LIMIT with the bracket of its last check."""
+        st = self._lib.reform_pria_set_time_limit(self._h, float(seconds))
+        if st != 0:
+            raise RuntimeError(f"reform_pria_set_time_limit failed with status {st}")
+
     def set_warm(self, x, y, z) -> None:
         self._warm = [np.ascontiguousarray(a, np.float64) for a in (x, y, z)]
         st = self._lib.reform_pria_set_warm(self._h, *[_native.dptr(a) for a in self._warm])
@@ -170,8 +181,12 @@ def solve(instance, *, tolerances: Tolerances = Tolerances(), time_limit: float 
           **schedule) -> JrpResult:
     """Solve the JRP LP of `instance` on the GPU (the reference backend's
     contract: only `tolerances.optimality` reaches the solver; `objective` is
-    the upper bound of an optimal run and NaN otherwise).  `time_limit` is
-    recorded; the solver's own budget is `max_iter`.  `precision` is "fp64" or
+    the upper bound of an optimal run and NaN otherwise).  `time_limit` is a
+    wall-clock budget in seconds for set-up and solve together, checked on the
+    host at every convergence check: past it the solve stops and the result is
+    status "time_limit" with the bracket of the last check (the reference's
+    backend instead kills its solver process, jrp/harness/backends/
+    pria_cuda.py:114-145, and records no bounds).  `precision` is "fp64" or
     "mixed" (FP32 iterates, FP64 reductions and bounds)."""
     common = dict(backend="pria-b200", instance=instance.name, family=instance.family,
                   items=instance.items, periods=instance.periods, entries=instance.entries,
@@ -190,16 +205,22 @@ def solve(instance, *, tolerances: Tolerances = Tolerances(), time_limit: float 
         return JrpResult(status="error", note=str(error)[:200], **common)
     setup = time.perf_counter() - start
     try:
+        if math.isfinite(time_limit):
+            dev.set_time_limit(max(0.0, time_limit - setup))
         start = time.perf_counter()
         st = dev.run()
         r = dev.result()
         seconds = time.perf_counter() - start
     finally:
         dev.close()
+    timed = dict(iterations=r.iterations, setup_seconds=setup, solve_seconds=seconds, **common)
+    if st == TIME_LIMIT:
+        return JrpResult(status="time_limit", lower=r.dual_objective, upper=r.primal_objective,
+                         note=f"stopped past the {time_limit:g}s limit at relative gap "
+                              f"{r.relative_gap:.3g}", **timed)
     if st != 0:
         return JrpResult(status="error", note=f"CUDA status {st}", setup_seconds=setup, **common)
     converged = math.isfinite(r.relative_gap) and r.relative_gap <= tolerances.optimality
-    timed = dict(iterations=r.iterations, setup_seconds=setup, solve_seconds=seconds, **common)
     if not converged:
         return JrpResult(status="iteration_limit", lower=r.dual_objective, upper=r.primal_objective,
                          note=f"relative gap {r.relative_gap:.3g}", **timed)
