@@ -736,8 +736,8 @@ __global__ void prep_edges_kernel(int m, const int* __restrict__ perm, const int
 }
 
 // ptr[v] = the first position p of the sorted `keys` with keys[p] >= v, v <= n.
-__global__ void prep_runs_kernel(int n, int m, const int* __restrict__ keys, int* __restrict__ ptr) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void prep_runs_kernel(long long n, int m, const int* __restrict__ keys, int* __restrict__ ptr) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // v = n is valid: n <= INT_MAX
     if (v > n) return;
     int lo = 0, hi = m;
     while (lo < hi) {
@@ -756,7 +756,7 @@ template <class Real>
 __global__ void prep_nodes_kernel(int n, const int* __restrict__ row_ptr, const int* __restrict__ col_ptr,
                                   const double* __restrict__ diag, const double* __restrict__ scale,
                                   Real* __restrict__ dn, Real* __restrict__ deg) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int incident = (row_ptr[i + 1] - row_ptr[i]) + (col_ptr[i + 1] - col_ptr[i]);
     deg[i] = Real(incident > 0 ? incident : 1);
@@ -905,8 +905,8 @@ struct Solver final : SolverBase {
         const int fl = *hflags;
         if (fl & 1) return PRAQ_ERROR_INSTANCE;
         if (ends.alloc(m, stream) || w.alloc(m, stream) || first.alloc(m, stream) ||
-            second.alloc(m, stream) || sidx.alloc(m, stream) || row_ptr.alloc(n + 1, stream) ||
-            col_ptr.alloc(n + 1, stream) || colidx.alloc(m, stream) || diag.alloc(n, stream) ||
+            second.alloc(m, stream) || sidx.alloc(m, stream) || row_ptr.alloc(size_t(n) + 1, stream) ||
+            col_ptr.alloc(size_t(n) + 1, stream) || colidx.alloc(m, stream) || diag.alloc(n, stream) ||
             deg.alloc(n, stream) || keys2.alloc(m, stream))
             return PRAQ_ERROR_CUDA;
         int key_bits = 1;
@@ -941,8 +941,8 @@ struct Solver final : SolverBase {
                 colidx.release();
             }
         }
-        prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, first.ptr, row_ptr.ptr);
-        prep_runs_kernel<<<ceil_div(n + 1, kBlock), kBlock, 0, stream>>>(n, m, keys2.ptr, col_ptr.ptr);
+        prep_runs_kernel<<<ceil_div((long long)n + 1, kBlock), kBlock, 0, stream>>>(n, m, first.ptr, row_ptr.ptr);
+        prep_runs_kernel<<<ceil_div((long long)n + 1, kBlock), kBlock, 0, stream>>>(n, m, keys2.ptr, col_ptr.ptr);
         prep_nodes_kernel<Real><<<ceil_div(n, kBlock), kBlock, 0, stream>>>(n, row_ptr.ptr, col_ptr.ptr, dg.ptr,
                                                                           scale.ptr, diag.ptr, deg.ptr);
         return cudaGetLastError() == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;

@@ -47,8 +47,10 @@ int reform_praq_create(const PraqInstance* instance, const PraqParameters* param
     (void)cudaGetLastError();   // a stale error of an unrelated earlier call is not ours
     PraqParameters p = *parameters;
     if (!praq::valid(p)) return PRAQ_ERROR_ARGUMENT;
+    // The reference's limits (qubo/praq-cuda/src/solver.cuh:525-526): node
+    // and edge ids are int32 on the device.
     const int64_t limit = std::numeric_limits<int>::max();
-    if (instance->n <= 0 || instance->n > limit / 32 || instance->m < 0 || instance->m > limit / 2)
+    if (instance->n <= 0 || instance->n > limit || instance->m < 0 || instance->m > limit / 2)
         return PRAQ_ERROR_INSTANCE;
     if (!instance->diag || (instance->m > 0 && (!instance->rows || !instance->cols || !instance->vals)))
         return PRAQ_ERROR_INSTANCE;
