@@ -123,6 +123,90 @@ REFORM_API int64_t reform_batch_launches(const reform_batch* b);
 
 REFORM_API void reform_batch_destroy(reform_batch* b);
 
+/* ---- the request server ------------------------------------------------- */
+
+/* A continuous-batching server over the engine above, with its own host
+ * thread (no counterpart in the reference; its in-library worker pattern is
+ * that of pria_solve_batch_*, jrp/pria-cuda/src/pria.cu:15-44).  Requests are
+ * submitted from any thread; the server admits them in arrival order while
+ * their estimated device bytes fit the budget (the first one always does),
+ * lays them out and starts them between block replays, keeps
+ * `blocks_in_flight` blocks queued, and marks converged requests finished
+ * after each block.  A finished request keeps its iterates on the device
+ * until it is retired; retiring returns its bytes to the budget.  With FP32
+ * iterates a QUBO whose gap has not halved over `stall_iterations`
+ * iterations continues in an FP64 engine from its last check (its result
+ * counts both phases' iterations).  All requests share the options'
+ * tolerance and max_iter.  Thread-safe, except that no call may overlap
+ * reform_server_destroy. */
+typedef struct reform_server reform_server;
+
+typedef struct {
+    int64_t budget_bytes;    /* device bytes admitted requests may hold (default 150e9) */
+    double tolerance;        /* relative gap (default 1e-4) */
+    int64_t max_iter;        /* per request (default 200000; < 0: none) */
+    int use_float32;         /* 1 (default): FP32 iterates, FP64 reductions; 0: FP64 */
+    int blocks_in_flight;    /* op_steps blocks queued on the GPU (default 2, at most 4) */
+    int admit_every;         /* while requests run, admission and retirement every this
+                                many blocks (default 4): each empties the pipeline once */
+    int stall_iterations;    /* FP32 QUBO plateau window (default 384; <= 0: never escalate) */
+} reform_server_options;
+
+/* A request's state.  Times in seconds since the server was created. */
+typedef struct {
+    int state;               /* 0 waiting, 1 running, 2 finished, 3 failed */
+    int error;               /* a failed request's error (as reform_batch_add_*) */
+    int kind;                /* 0 QUBO, 1 JRP */
+    int escalated;           /* 1: running or finished in the FP64 engine */
+    int64_t iterations;      /* at finish */
+    double lower, upper;     /* bracket at finish (instance units) */
+    double arrival, admitted, finished;   /* -1 until it happens */
+    int64_t device_bytes;    /* its share of the budget */
+} reform_server_request;
+
+typedef struct {
+    int64_t waiting, running, completed;
+    int64_t reserved_bytes, high_water_bytes;   /* budget in use now / at most */
+    int64_t device_bytes;                       /* held by the engines now */
+    int error;                                  /* nonzero: the loop stopped on this error */
+} reform_server_counts;
+
+REFORM_API reform_server_options reform_server_default_options(void);
+/* `options` may be NULL (the defaults); fields <= 0 take the defaults. */
+REFORM_API int reform_server_create(const reform_server_options* options, reform_server** out);
+
+/* Queue a request; its arrays are copied before the call returns.  Returns
+ * the request id (>= 0) or a negative error. */
+REFORM_API int64_t reform_server_submit_qubo(reform_server* s, const PraqInstance* instance);
+REFORM_API int64_t reform_server_submit_jrp(reform_server* s, int64_t n, int64_t t, const double* order_costs,
+                                            double joint_cost, const double* holding_costs);
+REFORM_API int64_t reform_server_submit_jrp_demand(reform_server* s, int64_t n, int64_t t,
+                                                   const double* order_costs, double joint_cost,
+                                                   const double* rate, const double* demand);
+
+/* Ids of requests that finished (or failed) since the last poll: up to `max`
+ * into `ids`, their number into *count; each id is reported once.  Waits up to
+ * `wait_seconds` for one when there is none.  Returns 0, or the loop's error. */
+REFORM_API int reform_server_poll(reform_server* s, int64_t* ids, int max, int* count, double wait_seconds);
+
+REFORM_API int reform_server_status(reform_server* s, int64_t id, reform_server_request* out);
+
+/* Results of a finished request (any output may be NULL), as
+ * reform_batch_result_qubo / _jrp. */
+REFORM_API int reform_server_result_qubo(reform_server* s, int64_t id, double* x, PraqResult* result);
+REFORM_API int reform_server_result_jrp(reform_server* s, int64_t id, double* x, double* y, double* z,
+                                        pria_result_info* info);
+
+/* Drop a request: a queued one at once; otherwise its device memory and its
+ * share of the budget are released at the loop's next admission turn.  A
+ * running request is cancelled. */
+REFORM_API int reform_server_retire(reform_server* s, int64_t id);
+
+REFORM_API int reform_server_stats(reform_server* s, reform_server_counts* out);
+
+/* Stops the loop (requests still running are abandoned) and frees everything. */
+REFORM_API void reform_server_destroy(reform_server* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,25 @@ class ReformShapes(ctypes.Structure):
                 ("reserved", c_int * 6)]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("budget_bytes", c_int64), ("tolerance", c_double), ("max_iter", c_int64),
+                ("use_float32", c_int), ("blocks_in_flight", c_int), ("admit_every", c_int),
+                ("stall_iterations", c_int)]
+
+
+class ServerRequest(ctypes.Structure):
+    _fields_ = [("state", c_int), ("error", c_int), ("kind", c_int), ("escalated", c_int),
+                ("iterations", c_int64), ("lower", c_double), ("upper", c_double),
+                ("arrival", c_double), ("admitted", c_double), ("finished", c_double),
+                ("device_bytes", c_int64)]
+
+
+class ServerCounts(ctypes.Structure):
+    _fields_ = [("waiting", c_int64), ("running", c_int64), ("completed", c_int64),
+                ("reserved_bytes", c_int64), ("high_water_bytes", c_int64),
+                ("device_bytes", c_int64), ("error", c_int)]
+
+
 _lib = None
 
 
@@ -127,6 +146,18 @@ def _declare(lib):
         "reform_batch_restart": (I, [V]),
         "reform_batch_launches": (c_int64, [V]),
         "reform_batch_destroy": (None, [V]),
+        "reform_server_default_options": (ServerOptions, []),
+        "reform_server_create": (I, [P(ServerOptions), P(V)]),
+        "reform_server_submit_qubo": (c_int64, [V, P(PraqInstance)]),
+        "reform_server_submit_jrp": (c_int64, [V, c_int64, c_int64, D, c_double, D]),
+        "reform_server_submit_jrp_demand": (c_int64, [V, c_int64, c_int64, D, c_double, D, D]),
+        "reform_server_poll": (I, [V, P(c_int64), I, P(c_int), c_double]),
+        "reform_server_status": (I, [V, c_int64, P(ServerRequest)]),
+        "reform_server_result_qubo": (I, [V, c_int64, D, P(PraqResult)]),
+        "reform_server_result_jrp": (I, [V, c_int64, D, D, D, P(PriaResultInfo)]),
+        "reform_server_retire": (I, [V, c_int64]),
+        "reform_server_stats": (I, [V, P(ServerCounts)]),
+        "reform_server_destroy": (None, [V]),
     })
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

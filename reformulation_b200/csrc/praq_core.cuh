@@ -888,8 +888,8 @@ struct Solver final : SolverBase {
         PoolBuf<double> vals, dg, part;
         PoolBuf<int> krow, kcol, first, second, sidx, flags, keys2, iota, ksorted;
         PoolBuf<unsigned char> temp;
-        if (dg.upload(in.diag, n, stream) || rows.upload(in.rows, m, stream) ||
-            cols.upload(in.cols, m, stream) || vals.upload(in.vals, m, stream) ||
+        if (upload_input(dg, in.diag, n) || upload_input(rows, in.rows, m) ||
+            upload_input(cols, in.cols, m) || upload_input(vals, in.vals, m) ||
             krow.alloc(m, stream) || kcol.alloc(m, stream) || flags.alloc(1, stream) ||
             part.alloc(kPrepBlocks, stream) || scale.alloc(1, stream))
             return PRAQ_ERROR_CUDA;
@@ -1037,6 +1037,19 @@ struct Solver final : SolverBase {
         node_kernel<Real, false, true, false, P><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.pred1, 0, 1, 0);
         lower_kernel<Real, false, P><<<nb_node, kBlock, 0, stream>>>(d, d.pred, d.pred1);
         if (m) edge_kernel<Real, false, true, P><<<nb_edge, kBlock, 0, stream>>>(d, d.pred, 0, 1, 0);
+    }
+
+    // Host -> device copy of one of the caller's (pageable) instance arrays:
+    // the driver's own pageable copy, or the library's pinned staging ring
+    // (host threads fill one slot while the copy engine drains the other).
+    // REFORM_PRAQ_UPLOAD=staged|direct in the environment picks one (for
+    // measurements); the default is the driver's copy.
+    template <class T>
+    cudaError_t upload_input(PoolBuf<T>& b, const T* host, size_t count) {
+        const char* env = std::getenv("REFORM_PRAQ_UPLOAD");
+        if (!(env && !std::strcmp(env, "staged"))) return b.upload(host, count, stream);
+        RB_CUDA_TRY(b.alloc(count, stream));
+        return staged_upload(b.ptr, host, sizeof(T) * count, stream);
     }
 
     // Slot-1 layout for m edges: pull once the step's edge arrays (ends, w,

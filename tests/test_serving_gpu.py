@@ -75,3 +75,56 @@ def test_budget_limits_admission(native):
     assert len(done) == len(reqs)
     # never more than what one (or two small) instances need was held at once
     assert server.high_water <= 3 * small
+
+
+def test_server_c_abi_poll_retire_and_cancel(native):
+    """The request server through its C ABI: requests submitted from the host
+    finish in the server's own thread, poll returns each id once, a finished
+    request's result equals the solo FP32 solve, retiring returns its bytes
+    to the budget, and a request retired while queued or running is
+    cancelled without disturbing the others."""
+    import ctypes
+    from ctypes import c_int, c_int64, c_void_p
+
+    from reformulation_b200 import _native, praq
+    L = _native.lib()
+    opts = L.reform_server_default_options()
+    opts.budget_bytes = int(4e9)
+    h = c_void_p()
+    assert L.reform_server_create(ctypes.byref(opts), ctypes.byref(h)) == 0
+    qs = [qubo_uniform_edges(200 + k, 400 + 300 * k, 3000 + 1000 * k) for k in range(5)]
+    big = qubo_uniform_edges(299, 40_000, 600_000)
+    views = [praq._View(q) for q in qs + [big]]
+    sids = [L.reform_server_submit_qubo(h, ctypes.byref(v.struct)) for v in views]
+    assert sids == list(range(6))
+    assert L.reform_server_retire(h, sids[-1]) == 0
+    ids = (c_int64 * 16)()
+    count = c_int(0)
+    seen = []
+    for _ in range(600):
+        assert L.reform_server_poll(h, ids, 16, ctypes.byref(count), 0.05) == 0
+        seen += [ids[k] for k in range(count.value)]
+        if set(sids[:5]) <= set(seen):
+            break
+    assert sorted(s for s in seen if s < 5) == sids[:5] and len(seen) == len(set(seen))
+    lib = praq.Library()
+    for q, sid in zip(qs, sids):
+        x = np.empty(q.n)
+        r = _native.PraqResult()
+        assert L.reform_server_result_qubo(h, sid, _native.dptr(x), ctypes.byref(r)) == 0
+        s = lib.solve(q, lib.parameters(tolerance=1e-4, use_float32=1, max_iter=200_000))
+        assert (r.iterations, r.lower, r.upper) == (s.iterations, s.lower, s.upper)
+        assert np.array_equal(x, s.x)
+        st = _native.ServerRequest()
+        assert L.reform_server_status(h, sid, ctypes.byref(st)) == 0
+        assert st.state == 2 and st.finished >= st.admitted >= st.arrival >= 0
+        assert L.reform_server_retire(h, sid) == 0
+    c = _native.ServerCounts()
+    for _ in range(400):                                     # removals happen in the loop
+        assert L.reform_server_stats(h, ctypes.byref(c)) == 0
+        if c.reserved_bytes == 0 and c.running == 0:
+            break
+        L.reform_server_poll(h, ids, 16, ctypes.byref(count), 0.01)
+    assert c.reserved_bytes == 0 and c.running == 0 and c.completed >= 5 and c.error == 0
+    assert c.high_water_bytes > 0
+    L.reform_server_destroy(h)
