@@ -511,10 +511,11 @@ def sub_batch(timer, steps, warmup, skip_cpu, qubos=256, jrps=128, autotune=True
                 "scaling": "strong", "n_gpus": world, "ms_per_step": step_max, "steps": steps,
                 "instances": n_all, "instances_this_rank": len(items), "shapes": shapes,
                 "gpu_launches_this_rank": int(launches)}
-    its, gaps, alg = [], [], 0.0
+    its, gaps, alg, uppers = [], [], 0.0, []
     for (kind, x), i in zip(items, ids):
         done, it, lo, up = b.status(i)
         its.append(it)
+        uppers.append(up)
         gaps.append((up - lo) / (1 + abs(up) + abs(lo)))
         alg += it * (praq_bytes(x.n, x.edges, 4)["iteration"] if kind == "qubo"
                      else pria_bytes(x.entries, 4)["iteration"])
@@ -526,7 +527,7 @@ def sub_batch(timer, steps, warmup, skip_cpu, qubos=256, jrps=128, autotune=True
     value = 1e3 * total / step_ms
 
     # plain FP64, one instance at a time
-    fp64_ms = {}
+    fp64_ms, fp64_upper = {}, {}
     for k, (kind, x) in enumerate(items):
         if k % fp64_stride:
             continue
@@ -538,8 +539,11 @@ def sub_batch(timer, steps, warmup, skip_cpu, qubos=256, jrps=128, autotune=True
                                     stream=stream.cuda_stream)
         dev.run()
         fp64_ms[k] = timer.solves(dev.run, 1)[0]
+        r64 = dev.result()
+        fp64_upper[k] = r64.upper if kind == "qubo" else r64.primal_objective
         dev.close()
     fp64_value = 1e3 * len(fp64_ms) / sum(fp64_ms.values())
+    diffs = [rel(uppers[k], fp64_upper[k]) for k in fp64_upper]
 
     # per size class: the class alone in a batch, against its FP64 solves
     classes = {}
@@ -573,6 +577,11 @@ def sub_batch(timer, steps, warmup, skip_cpu, qubos=256, jrps=128, autotune=True
                           "note": "every instance solved alone by the FP64 single-instance solver, "
                                   "device-resident, event-timed"},
            "batched_vs_plain_fp64": value / fp64_value,
+           "objective_vs_plain_fp64": {
+               "max_rel": max(diffs), "median_rel": pct(diffs, 50),
+               "above_1e-6": int(sum(d > 1e-6 for d in diffs)), "instances": len(diffs),
+               "note": "each instance's batched FP32-iterate objective (upper bound) against the "
+                       "plain FP64 single-instance solve, both to a 1e-4 gap"},
            "per_class": per_class,
            "roofline": {"bound": "hbm", "kernel": "all batched kernels over a whole step",
                         "achieved": alg / (step_ms / 1e3) / 1e9, "peak": peak[0], "unit": "GB/s",
@@ -854,7 +863,7 @@ def run_ours(args):
                         ("praq_n2e6", lambda: sub_praq_n2e6(timer, sub_steps, args.skip_cpu)),
                         ("pria", lambda: sub_pria(timer, sub_steps, args.skip_cpu)),
                         ("batch", lambda: sub_batch(timer, 3, 2, args.skip_cpu)),
-                        ("serving", lambda: sub_serving([100, 1000], 8.0, 2.0))):
+                        ("serving", lambda: sub_serving([50, 100], 8.0, 2.0))):
             t0 = time.perf_counter()
             try:
                 line[key] = fn()
