@@ -277,6 +277,11 @@ template <class Real>
 struct Engine final : EngineBase {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // Instances are laid out on their own stream, so that a layout (uploads,
+    // sorts, packing) overlaps the blocks already queued on `stream`; the
+    // engine's stream then waits for it before the instance is started.
+    cudaStream_t lay = nullptr;
+    cudaEvent_t lay_done = nullptr;
     int sms = 148;
     int op_steps = 0;
     Shapes shapes;
@@ -340,6 +345,11 @@ struct Engine final : EngineBase {
         }
         q.clear();
         j.clear();
+        if (lay) {   // the instances' buffers were freed on the layout stream
+            cudaStreamSynchronize(lay);
+            cudaStreamDestroy(lay);
+        }
+        if (lay_done) cudaEventDestroy(lay_done);
         // every stream-ordered free before the stream goes away
         qdevs.buf.release();
         qmeta.buf.release();
@@ -369,6 +379,9 @@ struct Engine final : EngineBase {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaStreamCreateWithFlags(&lay, cudaStreamNonBlocking) ||
+            cudaEventCreateWithFlags(&lay_done, cudaEventDisableTiming))
+            return -int(cudaErrorUnknown);
         if (counts.alloc(kCounts, stream)) return -int(cudaErrorMemoryAllocation);
         events.resize(4);
         for (auto& ev : events)
@@ -385,8 +398,9 @@ struct Engine final : EngineBase {
         auto s = std::make_unique<praq::Solver<Real>>();
         s->p = p;
         s->allow_pull = false;   // the engine's kernels read slot 1 in the push layout
-        const int st = s->setup(in, stream);
+        const int st = s->setup(in, lay);
         if (st) return st;
+        if (joined(s->stream)) return PRAQ_ERROR_CUDA;
         q.push_back(QInst{std::move(s)});
         ids.emplace_back(0, int(q.size()) - 1);
         dirty = true;
@@ -400,9 +414,10 @@ struct Engine final : EngineBase {
         if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
         p.op_steps = op_steps;
         std::unique_ptr<pria::SolverBase> base;
-        const int st = pria::create<double>(n, t, k, k0, h, &p, sizeof(Real) == 4, stream, base);
+        const int st = pria::create<double>(n, t, k, k0, h, &p, sizeof(Real) == 4, lay, base);
         if (st) return -st;
         std::unique_ptr<pria::Solver<Real>> s(static_cast<pria::Solver<Real>*>(base.release()));
+        if (joined(s->stream)) return -int(cudaErrorUnknown);
         j.push_back(JInst{std::move(s)});
         ids.emplace_back(1, int(j.size()) - 1);
         dirty = true;
@@ -416,13 +431,25 @@ struct Engine final : EngineBase {
         if (op_steps == 0) op_steps = std::max(p.op_steps, 2);
         p.op_steps = op_steps;
         std::unique_ptr<pria::SolverBase> base;
-        const int st = pria::create_demand(n, t, k, k0, rate, demand, &p, sizeof(Real) == 4, stream, base);
+        const int st = pria::create_demand(n, t, k, k0, rate, demand, &p, sizeof(Real) == 4, lay, base);
         if (st) return -st;
         std::unique_ptr<pria::Solver<Real>> s(static_cast<pria::Solver<Real>*>(base.release()));
+        if (joined(s->stream)) return -int(cudaErrorUnknown);
         j.push_back(JInst{std::move(s)});
         ids.emplace_back(1, int(j.size()) - 1);
         dirty = true;
         return int(ids.size()) - 1;
+    }
+
+    // A freshly laid-out instance joins the engine's stream: the stream waits
+    // for its layout, and every later operation of the instance (its start,
+    // result reads, warm starts) is ordered on the engine's stream.  Its
+    // buffers keep freeing on the layout stream, which happens only after the
+    // engine's stream has been drained (remove, destruction).
+    int joined(cudaStream_t& solver_stream) {
+        if (cudaEventRecord(lay_done, lay) || cudaStreamWaitEvent(stream, lay_done, 0)) return 1;
+        solver_stream = stream;
+        return 0;
     }
 
     template <class T>
@@ -603,7 +630,7 @@ struct Engine final : EngineBase {
 
     template <bool R, bool C>
     cudaError_t launch_yz(int c, int step, int gate, cudaStream_t st) {
-        constexpr int kT = pria::kZThreads;
+        constexpr int kT = pria::z_threads<Real>();
         const int per_sm = std::max(1, int((228 * 1024) / (yz_smem[c] + 4096)));
         const int nclusters = std::max(1, (sms * std::min(per_sm, 2)) / c);
         cudaLaunchConfig_t cfg = {};
@@ -642,9 +669,9 @@ struct Engine final : EngineBase {
         RB_CUDA_TRY(yattr(bj_y<Real, true, false>));
         RB_CUDA_TRY(yattr(bj_y<Real, true, true>));
         RB_CUDA_TRY(yattr(bj_y<Real, false, true>));
-        constexpr int kT = pria::kZThreads;
+        constexpr int kT = pria::z_threads<Real>();
         auto ya = [&](auto fn) -> cudaError_t {
-            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pria::kSliceBytes));
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pria::z_slice_bytes<Real>()));
             return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         };
         RB_CUDA_TRY(ya(bj_z<Real, kT, true, false>));

@@ -66,7 +66,18 @@ constexpr int kLowTW = 32;              // columns per tile of the lower-bound p
 #define RB200_PRIA_XTILE 8              // compile-time tunable (sweeps build with -D)
 #endif
 constexpr int kXTile = RB200_PRIA_XTILE;   // columns per tile of the x half-step (FP64 tile)
-constexpr int kSliceBytes = 96 * 1024;  // z slice per CTA of a cluster (two CTAs per SM)
+// z half-step CTA: threads and the shared-memory slice of a period block it
+// holds, per precision (compile-time tunables; sweeps build with -D).
+// Measured per solve (PRIA N = 100, T = 500 / N = 200, T = 300 / N = 60,
+// T = 200): FP64 with 256 threads 46.5 / 35.9 / 6.0 ms against 52.6 / 39.2 /
+// 5.9 with 512; FP32 with 512 threads and 96 KB slices 32.3 / 27.2 / 5.3 ms
+// (256 threads and 48 KB: 31.8 / 26.4 / 5.7).
+#ifndef RB200_PRIA_ZSLICE_KB
+#define RB200_PRIA_ZSLICE_KB 96
+#endif
+#ifndef RB200_PRIA_ZSLICE_KB_F64
+#define RB200_PRIA_ZSLICE_KB_F64 96
+#endif
 constexpr int kMaxCluster = 16;
 // rows per warp in flight (x kernel): 6 in FP32, 4 in FP64 (measured best
 // of 2, 3, 4, 6, 8 for each; 6 in FP64 and 8 in either hold too many registers)
@@ -78,7 +89,18 @@ constexpr int kZUnroll = 8;          // z elements per thread in flight (z kerne
 template <class Real>
 constexpr int y_chunk() { return sizeof(Real) == 4 ? 8 : 4; }
 constexpr int kYThreads = 256;       // y kernel: one warp per row, kYThreads / 32 rows per tile
-constexpr int kZThreads = 512;       // z kernel CTA
+#ifndef RB200_PRIA_ZTHREADS
+#define RB200_PRIA_ZTHREADS 512
+#endif
+#ifndef RB200_PRIA_ZTHREADS_F64
+#define RB200_PRIA_ZTHREADS_F64 256
+#endif
+template <class Real>
+constexpr int z_threads() { return sizeof(Real) == 8 ? RB200_PRIA_ZTHREADS_F64 : RB200_PRIA_ZTHREADS; }
+template <class Real>
+constexpr int z_slice_bytes() {
+    return (sizeof(Real) == 8 ? RB200_PRIA_ZSLICE_KB_F64 : RB200_PRIA_ZSLICE_KB) * 1024;
+}
 
 struct Control {
     double omega, theta, fp_error, check_error;
@@ -512,6 +534,44 @@ struct MichelotSteps {
     }
 };
 
+// Sums of K values over every thread of every CTA of a cluster, bitwise the
+// same on every CTA, with one cluster barrier: each warp's total goes to its
+// slot of slots[parity]; after the barrier warp 0 of each CTA adds all ranks'
+// slots (lane l takes slots l, l + 32, ... in order, then a shuffle tree, the
+// same on every CTA) and one CTA barrier hands the totals to every thread.
+// A round may reuse slots[parity] two rounds later: the barrier of the round
+// between them is reached by every warp 0 only after its reads.
+template <int K, int kWarps>
+__device__ __forceinline__ void cluster_sums(const double (&v)[K], double (*slots)[kWarps][K], double* tot,
+                                             int parity, cg::cluster_group& cluster, int csize,
+                                             double (&out)[K]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double w = warp_sum(v[k]);
+        if (lane == 0) slots[parity][warp][k] = w;
+    }
+    cluster.sync();
+    if (warp == 0) {
+        double a[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) a[k] = 0.0;
+        for (int idx = lane; idx < csize * kWarps; idx += 32) {
+            const double* pp = cluster.map_shared_rank(&slots[parity][idx % kWarps][0], idx / kWarps);
+#pragma unroll
+            for (int k = 0; k < K; ++k) a[k] += pp[k];
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            a[k] = warp_sum(a[k]);
+            if (lane == 0) tot[parity * K + k] = a[k];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = tot[parity * K + k];
+}
+
 // z half-step (solver.py:423) for period block s, one cluster of `csize` CTAs
 // per block; CTA `rank` owns rows [r0, r1) of the block, a contiguous slice.
 // z + r of the slice goes to shared memory, the threshold of the whole block
@@ -529,7 +589,8 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
     const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* vz = reinterpret_cast<Real*>(smem_raw);
-    __shared__ double part[2][2];
+    __shared__ double slots[2][kThreads / 32][2];
+    __shared__ double tot[2 * 2];
     __shared__ double scratch[3 * 32];
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
@@ -579,20 +640,10 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
                 b[1] += 1.0;
             }
         }
-        block_sums<2>(b, scratch, b);
-        if (threadIdx.x == 0) {
-            part[parity][0] = b[0];
-            part[parity][1] = b[1];
-        }
-        cluster.sync();
-        double s0 = 0.0, c0 = 0.0;
-        for (int rk = 0; rk < csize; ++rk) {
-            const double* pp = cluster.map_shared_rank(&part[parity][0], rk);
-            s0 += pp[0];
-            c0 += pp[1];
-        }
-        S = s0;
-        C = int(c0);
+        double t[2];
+        cluster_sums<2, kThreads / 32>(b, slots, tot, parity, cluster, csize, t);
+        S = t[0];
+        C = int(t[1]);
         parity ^= 1;
     };
     const double thz = michelot(active, d.n * len, double(d.k0), d.thz[s]);
@@ -659,7 +710,8 @@ __device__ __forceinline__ void z_task_pair(const Dev<Real>& d, int pair, const 
     const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* vz = reinterpret_cast<Real*>(smem_raw);
-    __shared__ double part[2][4];
+    __shared__ double slots[2][kThreads / 32][4];
+    __shared__ double tots[2 * 4];
     __shared__ double scratch[6 * 32];
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
@@ -731,18 +783,8 @@ __device__ __forceinline__ void z_task_pair(const Dev<Real>& d, int pair, const 
                 }
             }
         }
-        block_sums<4>(b, scratch, b);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) part[parity][k] = b[k];
-        }
-        cluster.sync();
-        double tot[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int rk = 0; rk < csize; ++rk) {
-            const double* pp = cluster.map_shared_rank(&part[parity][0], rk);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) tot[k] += pp[k];
-        }
+        double tot[4];
+        cluster_sums<4, kThreads / 32>(b, slots, tots, parity, cluster, csize, tot);
 #pragma unroll
         for (int g = 0; g < 2; ++g)
             if (!ms[g].done()) ms[g].feed(tot[2 * g], int(tot[2 * g + 1]));
@@ -811,7 +853,7 @@ z_kernel(Dev<Real> d, const Real* zsrc, int step, int gate) {
 // natural 56): 2-3.5 % faster PRIA solves at T >= 500, neutral below; in FP64
 // the cap spills and was 2-4 % slower, so z_kernel<double> keeps its own.
 template <int kThreads, bool Reflect, bool Check, bool Pair>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 1536 / kThreads)
 z_kernel_f32(Dev<float> d, const float* zsrc, int step, int gate) {
     if constexpr (Pair)
         z_task_pair<float, kThreads, Reflect, Check>(d, int(blockIdx.x) / d.csize, zsrc, step, gate);
@@ -1346,7 +1388,7 @@ struct Solver final : SolverBase {
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
-    static constexpr int kZThreadsPerCta = kZThreads;
+    static constexpr int kZThreadsPerCta = z_threads<Real>();
     // y rows: one padded row of at most kMaxPeriods reals per warp
     static constexpr size_t y_smem_limit() { return size_t(kYThreads / 32) * kMaxPeriods * sizeof(Real); }
     // x tiles: kXTile columns of a padded row of at most kMaxPeriods (+1)
@@ -1476,7 +1518,7 @@ struct Solver final : SolverBase {
         // grids under a wave, pairs are 1-7 % slower.
         auto cluster_for = [&](int row) {
             int c = 1;
-            while (c < kMaxCluster && size_t((n + c - 1) / c) * row * sizeof(Real) > size_t(kSliceBytes)) ++c;
+            while (c < kMaxCluster && size_t((n + c - 1) / c) * row * sizeof(Real) > size_t(z_slice_bytes<Real>())) ++c;
             return c > n ? n : c;
         };
         int zrow = tp + 1, csize = cluster_for(tp + 1);
@@ -1495,7 +1537,7 @@ struct Solver final : SolverBase {
         }
         yz_smem = size_t((n + csize - 1) / csize) * zrow * sizeof(Real);
         d.zstaged = 1;
-        if (yz_smem > size_t(kSliceBytes)) {   // the largest block exceeds a full cluster's slices
+        if (yz_smem > size_t(z_slice_bytes<Real>())) {   // the largest block exceeds a full cluster's slices
             d.zstaged = 0;
             yz_smem = 0;
         }
@@ -1553,8 +1595,8 @@ struct Solver final : SolverBase {
     cudaError_t yz_attr() {
         RB_CUDA_TRY(cudaFuncSetAttribute(y_kernel<Real, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(y_smem_limit())));
-        for (auto fn : {z_entry<Real, kZThreads, R, C, false>(), z_entry<Real, kZThreads, R, C, true>()}) {
-            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kSliceBytes));
+        for (auto fn : {z_entry<Real, z_threads<Real>(), R, C, false>(), z_entry<Real, z_threads<Real>(), R, C, true>()}) {
+            RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, z_slice_bytes<Real>()));
             RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         }
         return cudaSuccess;
@@ -1596,7 +1638,7 @@ struct Solver final : SolverBase {
         RB_CUDA_TRY(cudaGetLastError());
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(unsigned(z_tasks() * d.csize));   // a cluster per z task
-        cfg.blockDim = dim3(kZThreads);
+        cfg.blockDim = dim3(z_threads<Real>());
         cfg.dynamicSmemBytes = yz_smem;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
@@ -1606,8 +1648,8 @@ struct Solver final : SolverBase {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        if (d.zpair) return cudaLaunchKernelEx(&cfg, z_entry<Real, kZThreads, R, C, true>(), d, zs, step, gate);
-        return cudaLaunchKernelEx(&cfg, z_entry<Real, kZThreads, R, C, false>(), d, zs, step, gate);
+        if (d.zpair) return cudaLaunchKernelEx(&cfg, z_entry<Real, z_threads<Real>(), R, C, true>(), d, zs, step, gate);
+        return cudaLaunchKernelEx(&cfg, z_entry<Real, z_threads<Real>(), R, C, false>(), d, zs, step, gate);
     }
 
     cudaError_t launch_check(int mode) {
