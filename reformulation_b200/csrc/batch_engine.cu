@@ -59,10 +59,11 @@ enum Count { kNode = 0, kEdge, kQLow, kUp, kJLow, kQCheck, kJCheck, kY, kX0 };
 constexpr int kYZ0 = kX0 + kXClasses;
 constexpr int kMaxGroups = 17;   // y/z cluster sizes 1..16
 // JRPs of at least this many packed entries run their step kernels as their
-// own launches (the solo solver's grids, each instance a branch of the graph);
-// the smaller ones share the table-driven persistent kernels.
+// own launches (the solo solver's grids, one instance after the other on one
+// branch of the graph); the smaller ones share the table-driven persistent
+// kernels.
 constexpr long long kBigJrp = 1LL << 20;
-constexpr size_t kBigStream0 = 32;   // auxiliary streams of the big JRPs start here
+constexpr size_t kBigStream0 = 32;   // the auxiliary stream of the big JRPs' chain
 constexpr int kCounts = kYZ0 + kMaxGroups;
 
 // --- batched kernels: persistent grids over the work tables ---------------
@@ -781,24 +782,25 @@ struct Engine final : EngineBase {
                 for (size_t a = 1; a < k; ++a) RB_CUDA_TRY(order_after(aux[a], stream));
                 return cudaSuccess;
             };
-            // every big JRP runs its own step chain (the solo kernels) on its own
-            // branch, beside the table-driven chain of the small ones
+            // the big JRPs run their step chains (the solo kernels) one after
+            // the other on one branch, beside the table-driven chain of the
+            // small ones.  (One branch per big JRP, all concurrent, was slower:
+            // the batch workload's 15 JRPs above 10M entries took 1713 ms per
+            // step that way and 1500 ms in one chain; the whole batch 2700 ms
+            // against 2415 ms.)
             auto big_fork = [&]() -> cudaError_t {
-                for (size_t b = 0; b < jbig.size(); ++b) {
-                    cudaStream_t st;
-                    RB_CUDA_TRY(aux_stream(kBigStream0 + b, &st));
-                    RB_CUDA_TRY(order_after(stream, st));
-                }
-                return cudaSuccess;
+                if (jbig.empty()) return cudaSuccess;
+                cudaStream_t st;
+                RB_CUDA_TRY(aux_stream(kBigStream0, &st));
+                return order_after(stream, st);
             };
             auto big_join = [&]() -> cudaError_t {
-                for (size_t b = 0; b < jbig.size(); ++b) RB_CUDA_TRY(order_after(aux[kBigStream0 + b], stream));
-                return cudaSuccess;
+                return jbig.empty() ? cudaSuccess : order_after(aux[kBigStream0], stream);
             };
             RB_CUDA_TRY(big_fork());
             for (size_t b = 0; b < jbig.size(); ++b) {
                 auto& sv = *j[jbig[b]].s;
-                cudaStream_t st = aux[kBigStream0 + b];
+                cudaStream_t st = aux[kBigStream0];
                 for (int s = 0; s < op_steps; ++s) {
                     auto& dv = sv.d;
                     if (s + 1 < op_steps) {
@@ -833,7 +835,7 @@ struct Engine final : EngineBase {
             for (size_t b = 0; b < jbig.size(); ++b) {
                 auto& sv = *j[jbig[b]].s;
                 auto& dv = sv.d;
-                cudaStream_t st = aux[kBigStream0 + b];
+                cudaStream_t st = aux[kBigStream0];
                 RB_CUDA_TRY((sv.template launch_x<false, true>(dv.x2s, dv.y2s, dv.z2s, 0, 1, st)));
                 RB_CUDA_TRY((sv.template launch_yz<false, true>(dv.y2s, dv.z2s, 0, 1, st)));
                 nodes += 3;
@@ -866,9 +868,9 @@ struct Engine final : EngineBase {
         int ex = 0, eg = 0;
         for (bool b : xclasses) ex += b;
         for (bool b : groups) eg += b;
-        const size_t wide = std::max(size_t(std::max(ex, eg)) + 1, kBigStream0 + jbig.size());
+        const size_t wide = std::max(size_t(std::max(ex, eg)) + 1, kBigStream0 + (jbig.empty() ? 0 : 1));
         const size_t events_needed =
-            2 + size_t(op_steps + 1) * 2 * size_t(std::max(0, ex - 1) + eg) + 4 * jbig.size();
+            2 + size_t(op_steps + 1) * 2 * size_t(std::max(0, ex - 1) + eg) + 4;
         cudaStream_t tmp;
         if (aux_stream(wide, &tmp)) return -int(cudaErrorUnknown);
         while (fj.size() < events_needed) {
