@@ -641,7 +641,7 @@ def sub_batch(timer, steps, warmup, skip_cpu, qubos=256, jrps=128, autotune=True
     return out
 
 
-def sub_serving(rates, seconds, warm_s, pool_qubo=28, pool_jrp=12, tol=TOL):
+def sub_serving(rates, seconds, warm_s, pool_qubo=28, pool_jrp=12, tol=TOL, admit_every=None):
     """Config 5: Poisson arrivals (seed 4) at each rate for `seconds` after a
     `warm_s` warm-up stream, 70 % QUBO / 30 % JRP, instances drawn from a pool
     of the batch workload's size distributions; device-memory admission budget
@@ -676,7 +676,8 @@ def sub_serving(rates, seconds, warm_s, pool_qubo=28, pool_jrp=12, tol=TOL):
 
     rows = []
     for rate in rates:
-        server = serving.Server(budget_bytes=150e9, tolerance=tol)
+        server = serving.Server(budget_bytes=150e9, tolerance=tol,
+                                **({"admit_every": admit_every} if admit_every else {}))
         if warm_s > 0:
             warm, _ = stream_of(rate, warm_s, 40)
             server.serve(warm)
@@ -985,6 +986,8 @@ def main():
     ap.add_argument("--rates", type=float, nargs="+", default=[50, 100, 200, 500, 1000, 2000])
     ap.add_argument("--seconds", type=float, default=60.0)
     ap.add_argument("--warm-seconds", type=float, default=5.0)
+    ap.add_argument("--admit-every", type=int, default=None,
+                    help="serving: blocks between admissions while requests run")
     ap.add_argument("--profile-case", choices=("praq", "pria"))
     ap.add_argument("--n", type=int, default=100_000)
     ap.add_argument("--m", type=int, default=1_000_000)
@@ -1014,7 +1017,8 @@ def main():
                                                                not args.no_autotune, args.fp64_stride, rep))
     if args.workload == "serving":
         return _single(args, "serving", lambda t, rep: sub_serving(args.rates, args.seconds,
-                                                                   args.warm_seconds))
+                                                                   args.warm_seconds,
+                                                                   admit_every=args.admit_every))
     args.warmup = max(args.warmup, 3)
     return run_ours(args)
 

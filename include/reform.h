@@ -147,8 +147,8 @@ typedef struct {
     int64_t max_iter;        /* per request (default 200000; < 0: none) */
     int use_float32;         /* 1 (default): FP32 iterates, FP64 reductions; 0: FP64 */
     int blocks_in_flight;    /* op_steps blocks queued on the GPU (default 2, at most 4) */
-    int admit_every;         /* while requests run, admission and retirement every this
-                                many blocks (default 4): each empties the pipeline once */
+    int admit_every;         /* while requests run, admission and retirement at most every
+                                this many blocks (default 4; 1 measured the same) */
     int stall_iterations;    /* FP32 QUBO plateau window (default 384; <= 0: never escalate) */
 } reform_server_options;
 

@@ -218,12 +218,17 @@ bj_check(const pria::Dev<Real>* devs, const JMeta* metas, const int* __restrict_
     }
 }
 
-// Every instance's control block into one array (slot = instance slot).
+// Every running instance's control block into one array, at the instance's
+// id (ids are never reused, so a block captured before instances joined
+// still writes every instance it covers to the right place).
 template <class Real>
-__global__ void b_gather(const praq::Dev<Real>* qdevs, int nq, const pria::Dev<Real>* jdevs, int nj,
+__global__ void b_gather(const praq::Dev<Real>* qdevs, const int* __restrict__ qid, int nq,
+                         const pria::Dev<Real>* jdevs, const int* __restrict__ jid, int nj,
                          const unsigned char* __restrict__ live, Summary* out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nq + nj || !live[k]) return;
+    if (k >= nq + nj) return;
+    const int id = k < nq ? qid[k] : jid[k - nq];
+    if (!live[id]) return;
     Summary s;
     if (k < nq) {
         const praq::Control* c = qdevs[k].ctl;
@@ -232,7 +237,7 @@ __global__ void b_gather(const praq::Dev<Real>* qdevs, int nq, const pria::Dev<R
         const pria::Control* c = jdevs[k - nq].ctl;
         s = Summary{c->lower, c->upper, c->gap, c->iteration, c->terminated, c->restart};
     }
-    out[k] = s;
+    out[id] = s;
 }
 
 template <class T>
@@ -314,7 +319,8 @@ struct Engine final : EngineBase {
     Table<int2> t_x[kXClasses];
     Table<int2> t_yz[kMaxGroups];
     Table<int> l_qcheck, l_jcheck;
-    Table<unsigned char> live;
+    Table<int> qid_t, jid_t;          // QUBO / JRP index -> id
+    Table<unsigned char> live;        // per id: running in the current tables
     PoolBuf<int> counts;
     PoolBuf<Summary> summary;
     Summary* hsummary = nullptr;
@@ -346,6 +352,7 @@ struct Engine final : EngineBase {
         }
         q.clear();
         j.clear();
+        graves.clear();
         if (lay) {   // the instances' buffers were freed on the layout stream
             cudaStreamSynchronize(lay);
             cudaStreamDestroy(lay);
@@ -361,6 +368,8 @@ struct Engine final : EngineBase {
         for (auto& tb : t_yz) tb.buf.release();
         l_qcheck.buf.release();
         l_jcheck.buf.release();
+        qid_t.buf.release();
+        jid_t.buf.release();
         live.buf.release();
         counts.release();
         summary.release();
@@ -491,13 +500,17 @@ struct Engine final : EngineBase {
         for (auto& tb : t_yz) tb.host.clear();
         l_qcheck.host.clear();
         l_jcheck.host.clear();
-        live.host.assign(q.size() + j.size(), 0);
+        live.host.assign(ids.size(), 0);
+        qid_t.host.assign(q.size(), 0);
+        jid_t.host.assign(j.size(), 0);
+        for (int id = 0; id < int(ids.size()); ++id)
+            (ids[id].first == 0 ? qid_t.host[ids[id].second] : jid_t.host[ids[id].second]) = id;
         size_t ys[kMaxGroups] = {};
         bool gr[kMaxGroups] = {};
         for (int k = 0; k < int(q.size()); ++k) {
             auto& qi = q[k];
             if (!qi.s || !qi.started || qi.done) continue;
-            live.host[k] = 1;
+            live.host[qid_t.host[k]] = 1;
             for (int t = 0; t < qi.s->nb_node; ++t) {
                 t_node.host.push_back(make_int2(k, t));
                 t_qlow.host.push_back(make_int2(k, t));
@@ -512,7 +525,7 @@ struct Engine final : EngineBase {
         for (int k = 0; k < int(j.size()); ++k) {
             auto& ji = j[k];
             if (!ji.s || !ji.started || ji.done) continue;
-            live.host[q.size() + k] = 1;
+            live.host[jid_t.host[k]] = 1;
             auto& s = *ji.s;
             const int n = s.n, tp = s.tp, ntc = s.d.ntc;
             const bool big = s.nd >= kBigJrp;
@@ -579,7 +592,9 @@ struct Engine final : EngineBase {
             if (xclasses[c] && (rc = upload(t_x[c]))) return rc;
         for (int c = 1; c < kMaxGroups; ++c)
             if (groups[c] && (rc = upload(t_yz[c]))) return rc;
-        if ((rc = upload(l_qcheck)) || (rc = upload(l_jcheck)) || (rc = upload(live))) return rc;
+        if ((rc = upload(l_qcheck)) || (rc = upload(l_jcheck)) || (rc = upload(live)) || (rc = upload(qid_t)) ||
+            (rc = upload(jid_t)))
+            return rc;
         hcounts[kNode] = int(t_node.host.size());
         hcounts[kEdge] = int(t_edge.host.size());
         hcounts[kQLow] = int(t_qlow.host.size());
@@ -592,7 +607,7 @@ struct Engine final : EngineBase {
         for (int c = 0; c < kMaxGroups; ++c) hcounts[kYZ0 + c] = int(t_yz[c].host.size());
         if (cudaMemcpyAsync(counts.ptr, hcounts, sizeof(hcounts), cudaMemcpyHostToDevice, stream))
             return -int(cudaErrorUnknown);
-        const size_t slots = q.size() + j.size();
+        const size_t slots = ids.size();
         if (summary.count < slots) {
             if (summary.alloc(std::max<size_t>(slots * 2, 64), stream)) return -int(cudaErrorMemoryAllocation);
             dirty = true;
@@ -849,9 +864,10 @@ struct Engine final : EngineBase {
             nodes += 1;
         }
         if (hq && hj) RB_CUDA_TRY(order_after(sq, stream));
-        const int slots = int(q.size() + j.size());
-        b_gather<Real><<<std::max(1, ceil_div(slots, 128)), 128, 0, stream>>>(
-            qdevs.buf.ptr, int(q.size()), jdevs.buf.ptr, int(j.size()), live.buf.ptr, summary.ptr);
+        const int slots = int(ids.size());
+        b_gather<Real><<<std::max(1, ceil_div(int(q.size() + j.size()), 128)), 128, 0, stream>>>(
+            qdevs.buf.ptr, qid_t.buf.ptr, int(q.size()), jdevs.buf.ptr, jid_t.buf.ptr, int(j.size()), live.buf.ptr,
+            summary.ptr);
         nodes += 1;
         RB_CUDA_TRY(cudaMemcpyAsync(hsummary, summary.ptr, sizeof(Summary) * slots, cudaMemcpyDeviceToHost, stream));
         block_nodes = nodes;
@@ -887,12 +903,19 @@ struct Engine final : EngineBase {
         return 0;
     }
 
+    // Cold-start the instances added since the last call.  Their first step
+    // and check run on the layout stream, so the blocks already queued keep
+    // the GPU busy meanwhile (no drain): the engine's stream then waits for
+    // the layout stream, and the tables (uploaded on the engine's stream,
+    // behind the queued blocks) take the newcomers in from the next capture.
     int start() override {
-        if (pending && drain()) return -int(cudaErrorUnknown);
         for (auto& qi : q) {
             if (!qi.s || qi.started) continue;
+            qi.s->stream = lay;
             const int st = qi.s->start_solve();
+            qi.s->stream = stream;
             if (st) return st;
+            if (joined(qi.s->stream)) return PRAQ_ERROR_CUDA;
             qi.started = true;
             qi.join = launched;
             nlaunch += qi.s->launches();
@@ -902,8 +925,11 @@ struct Engine final : EngineBase {
         }
         for (auto& ji : j) {
             if (!ji.s || ji.started) continue;
+            ji.s->stream = lay;
             const cudaError_t st = ji.s->start_solve();
+            ji.s->stream = stream;
             if (st) return -int(st);
+            if (joined(ji.s->stream)) return -int(cudaErrorUnknown);
             ji.started = true;
             ji.join = launched;
             nlaunch += ji.s->launches();
@@ -921,9 +947,12 @@ struct Engine final : EngineBase {
         return a;
     }
 
+    // A new capture does not wait for the blocks in flight: they replay the
+    // old executable graph (freed when they finish), whose tables and slots
+    // stay valid (tables are rewritten on the stream behind them, summaries
+    // are written at instance ids).
     int launch() override {
         if (dirty) {
-            if (pending && drain()) return -int(cudaErrorUnknown);
             const int rc = capture();
             if (rc) return rc;
         }
@@ -942,7 +971,34 @@ struct Engine final : EngineBase {
         head = (head + pending) % int(events.size());
         synced += pending;
         pending = 0;
+        bury(true);
         return 0;
+    }
+
+    // Removed instances whose memory blocks still in flight may read (their
+    // control blocks and descriptors: those blocks skip them, but look);
+    // each is freed once every block enqueued before its removal has been
+    // synced.  Freed on the layout stream, so the host never waits for the
+    // engine's stream here.
+    struct Grave {
+        std::unique_ptr<praq::Solver<Real>> qs;
+        std::unique_ptr<pria::Solver<Real>> js;
+        long long after;   // blocks that must have been synced first
+    };
+    std::vector<Grave> graves;
+    void bury(bool all) {
+        for (size_t g = 0; g < graves.size();) {
+            if (all || graves[g].after <= synced) {
+                if (graves[g].qs) graves[g].qs->stream = lay;
+                if (graves[g].js) graves[g].js->stream = lay;
+                graves[g].qs.reset();
+                graves[g].js.reset();
+                graves[g] = std::move(graves.back());
+                graves.pop_back();
+            } else {
+                ++g;
+            }
+        }
     }
 
     int sync(int* out_ids, int max, int* count) override {
@@ -952,12 +1008,13 @@ struct Engine final : EngineBase {
         head = (head + 1) % int(events.size());
         --pending;
         const long long block = synced++;
+        bury(false);
         // the host copy holds the state after this block (or a later one)
         bool changed = false;
         int nout = 0;
         for (int id = 0; id < int(ids.size()); ++id) {
             const auto [kind, k] = ids[id];
-            const int slot = kind == 0 ? k : int(q.size()) + k;
+            const int slot = id;
             bool* done = kind == 0 ? &q[k].done : &j[k].done;
             const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
                                            : (j[k].s && j[k].started && !j[k].done);
@@ -1010,22 +1067,34 @@ struct Engine final : EngineBase {
         return 0;
     }
 
+    // A finished instance is read on the layout stream, with no wait for the
+    // blocks in flight: they skip it and write none of its memory, and the
+    // block that finished it is complete (the summary that said so was copied
+    // at its end).  An instance still running is read after a drain.
     int result_qubo(int id, double* x, PraqResult* r) override {
         if (id < 0 || id >= int(ids.size()) || ids[id].first != 0) return PRAQ_ERROR_ARGUMENT;
         auto& qi = q[ids[id].second];
         if (!qi.s) return PRAQ_ERROR_ARGUMENT;
-        if (pending && drain()) return PRAQ_ERROR_CUDA;
-        if (cudaMemcpyAsync(qi.s->mirror, qi.s->d.ctl, sizeof(praq::Control), cudaMemcpyDeviceToHost, stream) ||
-            cudaStreamSynchronize(stream))
+        if (!qi.done && pending && drain()) return PRAQ_ERROR_CUDA;
+        const cudaStream_t on = qi.done ? lay : stream;
+        if (cudaMemcpyAsync(qi.s->mirror, qi.s->d.ctl, sizeof(praq::Control), cudaMemcpyDeviceToHost, on) ||
+            cudaStreamSynchronize(on))
             return PRAQ_ERROR_CUDA;
-        return qi.s->result(x, nullptr, r);
+        qi.s->stream = on;
+        const int st = qi.s->result(x, nullptr, r);
+        qi.s->stream = stream;
+        return st;
     }
 
     int set_warm_qubo(int id, const double* x, const double* y2) override {
         if (id < 0 || id >= int(ids.size()) || ids[id].first != 0) return PRAQ_ERROR_ARGUMENT;
         auto& qi = q[ids[id].second];
         if (!qi.s || qi.started) return PRAQ_ERROR_ARGUMENT;
-        return qi.s->set_warm(x, y2);
+        // on the layout stream, where the instance will be started
+        qi.s->stream = lay;
+        const int st = qi.s->set_warm(x, y2);
+        qi.s->stream = stream;
+        return st;
     }
 
     // The point of the instance's last check (its bracket's primal and dual),
@@ -1045,23 +1114,42 @@ struct Engine final : EngineBase {
         if (id < 0 || id >= int(ids.size()) || ids[id].first != 1) return int(cudaErrorInvalidValue);
         auto& ji = j[ids[id].second];
         if (!ji.s) return int(cudaErrorInvalidValue);
-        if (pending && drain()) return int(cudaErrorUnknown);
-        if (cudaMemcpyAsync(ji.s->mirror, ji.s->d.ctl, sizeof(pria::Control), cudaMemcpyDeviceToHost, stream) ||
-            cudaStreamSynchronize(stream))
+        if (!ji.done && pending && drain()) return int(cudaErrorUnknown);
+        const cudaStream_t on = ji.done ? lay : stream;
+        if (cudaMemcpyAsync(ji.s->mirror, ji.s->d.ctl, sizeof(pria::Control), cudaMemcpyDeviceToHost, on) ||
+            cudaStreamSynchronize(on))
             return int(cudaErrorUnknown);
-        return ji.s->result(x, y, z, info);
+        ji.s->stream = on;
+        const int st = ji.s->result(x, y, z, info);
+        ji.s->stream = stream;
+        return st;
     }
 
     // A running instance leaves the work tables first (after the blocks in
-    // flight have finished); then its device memory is freed.
+    // flight have finished); then its device memory is freed.  A finished
+    // one (or one never started) is out of the tables already: its memory is
+    // freed once the blocks now in flight have been synced, with no wait.
     int remove(int id) override {
         if (id < 0 || id >= int(ids.size())) return PRAQ_ERROR_ARGUMENT;
         const auto [kind, k] = ids[id];
         const bool running = kind == 0 ? (q[k].s && q[k].started && !q[k].done)
                                        : (j[k].s && j[k].started && !j[k].done);
-        if (pending && drain()) return PRAQ_ERROR_CUDA;
-        if (kind == 0) q[k].s.reset(); else j[k].s.reset();
-        return running ? rebuild() : 0;
+        if (running) {
+            if (pending && drain()) return PRAQ_ERROR_CUDA;
+            if (kind == 0) q[k].s.reset(); else j[k].s.reset();
+            return rebuild();
+        }
+        if (pending) {
+            Grave g{};
+            if (kind == 0) g.qs = std::move(q[k].s); else g.js = std::move(j[k].s);
+            g.after = launched;
+            graves.push_back(std::move(g));
+        } else if (kind == 0) {
+            q[k].s.reset();
+        } else {
+            j[k].s.reset();
+        }
+        return 0;
     }
 
     int64_t device_bytes() const override {

@@ -292,8 +292,8 @@ struct Server {
                     waiting.push_back(incoming.front());
                     incoming.pop_front();
                 }
-                // admission (and removal) empty the pipeline once, so while
-                // requests run they happen every `admit_every` blocks
+                // while requests run, admission and removal happen at most
+                // every `admit_every` blocks
                 const bool turn = running == 0 || since_admit >= opt.admit_every;
                 if (turn && !retiring.empty()) retire_now.swap(retiring);
                 while (turn && !waiting.empty()) {

@@ -128,3 +128,21 @@ def test_server_c_abi_poll_retire_and_cancel(native):
     assert c.reserved_bytes == 0 and c.running == 0 and c.completed >= 5 and c.error == 0
     assert c.high_water_bytes > 0
     L.reform_server_destroy(h)
+
+
+def test_server_escalates_a_stalled_qubo_to_fp64(native, oracle_lib):
+    """FP32 iterates cannot reach a 1e-8 gap on this QUBO: the server's
+    plateau test moves it to its FP64 engine at its last check (status
+    `escalated`), where it finishes to 1e-8 and to the max-flow roof dual,
+    with the iterations of both phases.  (All of a server's requests share one
+    tolerance, and FP32 JRPs level off near 1e-6, so no JRP is served here.)"""
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.serving import Request, Server
+    q = qubo_uniform_edges(3, 700, 2000)
+    server = Server(budget_bytes=2e9, tolerance=1e-8, max_iter=400_000, stall_iterations=256)
+    done = server.serve([Request(0, 0.0, q)])
+    server.close()
+    assert len(done) == 1 and done[0].escalated
+    assert done[0].gap <= 1e-8 and done[0].iterations > 256
+    flow = oracle_lib.roof_dual_maxflow(q)
+    assert rel(done[0].upper, flow) <= 1e-7
