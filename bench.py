@@ -284,9 +284,18 @@ def sub_praq_n200(timer, steps, skip_cpu):
     for prec, f32 in (("fp64", 0), ("mixed", 1)):
         p = lib.parameters(tolerance=TOL, use_float32=f32)
         with praq.DeviceSolver(inst, p, stream=stream) as dev:
+            # the per-kernel graph first, for comparison; then the automatic
+            # choice (the persistent kernel at this size)
+            dev.set_megakernel(0)
+            for _ in range(5):
+                dev.run()
+            gms = timer.solves(dev.run, steps)
+            graph = {"p50_ms": pct(gms, 50), "p99_ms": pct(gms, 99), "launches_per_solve": dev.launches()}
+            persistent = dev.set_megakernel(-1)
             for _ in range(5):
                 dev.run()
             ms = timer.solves(dev.run, steps)
+            launches = dev.launches()
             res = dev.result(want_x=False)
             _, prof = dev.run_profiled()
         e2e = []
@@ -297,6 +306,7 @@ def sub_praq_n200(timer, steps, skip_cpu):
         assert s.status == 0
         alg = praq_bytes(inst.n, inst.edges, 8 if prec == "fp64" else 4)["iteration"]
         out[prec] = {"solves_per_s": 1e3 * len(ms) / sum(ms), "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99),
+                     "persistent_kernel": persistent, "launches_per_solve": launches, "graph": graph,
                      "e2e_solves_per_s": len(e2e) / sum(e2e), "e2e_p50_ms": 1e3 * pct(e2e, 50),
                      "e2e_p99_ms": 1e3 * pct(e2e, 99), "iterations": res.iterations,
                      "upper": res.upper, "relative_gap": res.gap,
@@ -305,8 +315,9 @@ def sub_praq_n200(timer, steps, skip_cpu):
     out["value"] = out["mixed"]["solves_per_s"]
     out["plain_fp64"] = {"value": out["fp64"]["solves_per_s"], "p50_ms": out["fp64"]["p50_ms"],
                          "p99_ms": out["fp64"]["p99_ms"]}
-    out["roofline"] = {"bound": "latency", "note": "30 KB of iterates: launch and dependency latency "
-                       "bound, not HBM; achieved_gbs_whole_solve gives bytes per second of a solve",
+    out["roofline"] = {"bound": "latency", "note": "30 KB of iterates: one CTA's dependency latency "
+                       "bound (the persistent kernel is a grid of one CTA here), not HBM; "
+                       "achieved_gbs_whole_solve gives bytes per second of a solve",
                        "achieved": out["mixed"]["achieved_gbs_whole_solve"], "peak": peaks()[0],
                        "unit": "GB/s", "frac": out["mixed"]["achieved_gbs_whole_solve"] / peaks()[0]}
     if not skip_cpu:
@@ -425,6 +436,73 @@ def sub_pria(timer, steps, skip_cpu):
                                          f"FP64 CPU restatement oracle/pria_oracle.c, {threads} OpenMP "
                                          f"threads, {t_block:.2f} s, scaled to the {iters} iterations of "
                                          "a full solve"}
+    return out
+
+
+def sub_pria_small(timer, steps, skip_cpu):
+    """Small JRPs, latency-bound: N=10, T=25 and N=30, T=75 (seeds 5, 6), to
+    1e-4.  Device-resident solves from the cold start with the solver's
+    automatic choice beside the per-kernel graph and the persistent kernel
+    (one cooperative launch per check block) forced on, mixed and FP64;
+    solves through pria_solve with host buffers; the CPU restatement on one
+    thread."""
+    from reformulation_b200 import pria
+    from reformulation_b200.instances import jrp_demand
+    lib = pria.Library()
+    stream = timer.stream.cuda_stream
+    out = {"workload": "PRIA JRP LP N=10 T=25 (seed 5) and N=30 T=75 (seed 6), demand-driven H, to 1e-4",
+           "unit": UNIT}
+    for n, t, seed in ((10, 25, 5), (30, 75, 6)):
+        inst = jrp_demand(seed, n, t)
+        p = lib.parameters(1_000_000, TOL)
+        rec = {"entries": inst.entries}
+        for prec in ("mixed", "fp64"):
+            for mode, name in ((-1, "auto"), (0, "graph"), (1, "persistent")):
+                with pria.DeviceSolver(inst, p, prec, stream=stream) as dev:
+                    active = dev.set_megakernel(mode)
+                    for _ in range(3):
+                        dev.run()
+                    ms = timer.solves(dev.run, steps)
+                    r = dev.result()
+                    launches = dev.launches()
+                rec[f"{prec}_{name}"] = {
+                    "persistent_kernel": active, "solves_per_s": 1e3 * len(ms) / sum(ms),
+                    "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99), "iterations": r.iterations,
+                    "upper": r.primal_objective, "relative_gap": r.relative_gap,
+                    "launches_per_solve": launches}
+        e2e = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            s = lib.solve(inst, p, precision="mixed")
+            e2e.append(time.perf_counter() - t0)
+            assert s.status == 0
+        rec["mixed_e2e"] = {"solves_per_s": len(e2e) / sum(e2e), "p50_ms": 1e3 * pct(e2e, 50),
+                            "p99_ms": 1e3 * pct(e2e, 99)}
+        rec["graph_over_persistent_p50"] = {
+            prec: rec[f"{prec}_graph"]["p50_ms"] / rec[f"{prec}_persistent"]["p50_ms"] for prec in ("mixed", "fp64")}
+        rec["mixed_vs_fp64_upper_rel"] = rel(rec["mixed_auto"]["upper"], rec["fp64_auto"]["upper"])
+        if not skip_cpu:
+            import oracle
+            tt = []
+            while sum(tt) < 2.0 and len(tt) < 50:
+                t0 = time.perf_counter()
+                ref = oracle.pria_solve(inst, oracle.pria_params(tolerance=TOL), threads=1)
+                tt.append(time.perf_counter() - t0)
+            rec["cpu_baseline"] = {"value": len(tt) / sum(tt), "unit": UNIT, "cores": 1, "kind": "port",
+                                   "sample": f"{len(tt)} FP64 solves to 1e-4 ({ref['iterations']} iterations) "
+                                             "by the CPU restatement oracle/pria_oracle.c, 1 thread",
+                                   "p50_ms": 1e3 * pct(tt, 50)}
+            rec["objective_check"] = {"oracle_fp64_upper": ref["upper"],
+                                      "fp64_rel_err": rel(rec["fp64_auto"]["upper"], ref["upper"]),
+                                      "mixed_rel_err": rel(rec["mixed_auto"]["upper"], ref["upper"])}
+        out[f"n{n}_t{t}"] = rec
+    big = out["n30_t75"]
+    out["value"] = big["mixed_auto"]["solves_per_s"]
+    out["plain_fp64"] = {"value": big["fp64_auto"]["solves_per_s"], "p50_ms": big["fp64_auto"]["p50_ms"]}
+    if "cpu_baseline" in big:
+        out["cpu_baseline"] = big["cpu_baseline"]
+    out["roofline"] = {"bound": "latency", "note": "under 2 MB of iterates, L2-resident: launch, barrier and "
+                       "dependency latency bound, not HBM"}
     return out
 
 
@@ -887,6 +965,7 @@ def run_ours(args):
         for key, fn in (("praq_n200", lambda: sub_praq_n200(timer, 50, args.skip_cpu)),
                         ("praq_n2e6", lambda: sub_praq_n2e6(timer, sub_steps, args.skip_cpu)),
                         ("pria", lambda: sub_pria(timer, sub_steps, args.skip_cpu)),
+                        ("pria_small", lambda: sub_pria_small(timer, 30, args.skip_cpu)),
                         ("batch", lambda: sub_batch(timer, 3, 2, args.skip_cpu)),
                         ("serving", lambda: sub_serving([50, 100], 8.0, 2.0))):
             t0 = time.perf_counter()
@@ -977,7 +1056,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline legs")
     ap.add_argument("--headline-only", action="store_true", help="omit the sub-objects")
-    ap.add_argument("--workload", choices=("default", "praq_n200", "praq_n2e6", "pria", "batch", "serving"),
+    ap.add_argument("--workload", choices=("default", "praq_n200", "praq_n2e6", "pria", "pria_small", "batch",
+                                           "serving"),
                     default="default", help="one workload alone (longer settings than the default line)")
     ap.add_argument("--qubos", type=int, default=256)
     ap.add_argument("--jrps", type=int, default=128)
@@ -1011,6 +1091,8 @@ def main():
         return _single(args, "praq_n2e6", lambda t, rep: sub_praq_n2e6(t, args.steps, args.skip_cpu))
     if args.workload == "pria":
         return _single(args, "pria", lambda t, rep: sub_pria(t, args.steps, args.skip_cpu))
+    if args.workload == "pria_small":
+        return _single(args, "pria_small", lambda t, rep: sub_pria_small(t, args.steps, args.skip_cpu))
     if args.workload == "batch":
         return _single(args, "batch", lambda t, rep: sub_batch(t, args.steps, max(args.warmup, 1),
                                                                args.skip_cpu, args.qubos, args.jrps,

@@ -124,12 +124,28 @@ REFORM_API int reform_praq_set_warm(reform_praq_solver* solver, const double* x,
 REFORM_API int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds);
 
 /* A measurement run: the same solve with every kernel launched on its own
- * between a pair of CUDA events on the solver's stream.  ms[9] and count[9]
+ * between a pair of CUDA events on the solver's stream.  ms[10] and count[10]
  * receive each kernel kind's total device milliseconds and launch count, in
  * this order: node step, edge step, node step with check sums, edge step with
  * check sums, lower-bound pass, check, restart node step, restart edge step,
- * restart check.  Returns the status like reform_praq_run. */
+ * restart check, and a whole check block of the persistent kernel (below).
+ * Returns the status like reform_praq_run. */
 REFORM_API int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* count);
+
+/* Small instances: a check block runs as ONE cooperative launch whose phases
+ * (node step; edge step; lower bound; check; restart step) are separated by
+ * grid barriers -- a grid of one CTA for a few hundred nodes -- in place of
+ * the captured graph of one kernel per phase.  No counterpart in the
+ * reference's praq-cuda; its pria-cuda has one (PRIA_MEGA).  `mode` -1:
+ * automatic (the default; on when a step's arrays take at most 2 MB), 0: off,
+ * 1: on whenever the instance allows it (the slot-1 push layout, i.e. edge
+ * arrays within twice the L2 size).  REFORM_PRAQ_MEGA=0|1 in the environment
+ * sets the mode at creation.  *active (may be NULL) receives 1 when later runs
+ * take the persistent kernel.  Results equal the graph's bit for bit (the same
+ * tile functions, CTA shape and sums).  Every barrier wait is bounded (1 s of
+ * device time): one that runs out ends the launch and the run returns
+ * PRAQ_ERROR_CUDA with the context still usable. */
+REFORM_API int reform_praq_set_megakernel(reform_praq_solver* solver, int mode, int* active);
 
 /* Kernel launches the last run issued (graph kernel nodes included). */
 REFORM_API int64_t reform_praq_launches(const reform_praq_solver* solver);

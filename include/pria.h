@@ -133,10 +133,27 @@ REFORM_API int reform_pria_result(reform_pria_solver* solver, double* x, double*
                                   pria_result_info* info);
 
 /* A measurement run: every kernel between a pair of CUDA events on the
- * solver's stream; ms[8]/count[8] receive each kind's total device time and
+ * solver's stream; ms[9]/count[9] receive each kind's total device time and
  * launches: x step, y/z step, x step with check sums, y/z step with check
- * sums, upper bound, lower bound, check, restart (x, y/z, check together). */
+ * sums, upper bound, lower bound, check, restart (x, y/z, check together),
+ * and a whole check block of the persistent kernel (below). */
 REFORM_API int reform_pria_run_profiled(reform_pria_solver* solver, double* ms, int64_t* count);
+
+/* Small instances (the reference's megakernel, jrp/pria-cuda/src/solver.cuh:
+ * 145-312, PRIA_MEGA): a check block runs as ONE cooperative launch whose
+ * phases (x; y and z; bounds; check; restart step) are separated by grid
+ * barriers, in place of the captured graph of one kernel per phase.  `mode`
+ * -1: automatic (the default; on for at most 16,384 packed entries, the sizes
+ * where it measured at least as fast as the graph), 0: off, 1: on whenever
+ * the instance allows it (every z period block within one CTA's shared
+ * memory).  The environment variable REFORM_PRIA_MEGA=0|1 sets the mode at
+ * creation.  *active (may be NULL) receives 1 when later runs take the
+ * persistent kernel.  Results equal the graph's bit for bit in FP64 (the same
+ * tile functions and sums); FP32 z sums are taken over 256-thread CTAs
+ * instead of 512, so low bits may differ.  Every barrier wait is bounded (1 s
+ * of device time): one that runs out ends the launch, and the run returns
+ * cudaErrorLaunchTimeout (702) with the context still usable. */
+REFORM_API int reform_pria_set_megakernel(reform_pria_solver* solver, int mode, int* active);
 
 REFORM_API int64_t reform_pria_launches(const reform_pria_solver* solver);
 

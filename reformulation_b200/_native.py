@@ -96,6 +96,7 @@ def _declare(lib):
         "reform_praq_set_time_limit": (I, [c_void_p, c_double]),
         "reform_praq_set_warm": (I, [c_void_p, P(c_double), P(c_double)]),
         "reform_praq_run_profiled": (I, [c_void_p, D, P(c_int64)]),
+        "reform_praq_set_megakernel": (I, [c_void_p, c_int, P(c_int)]),
         "reform_praq_launches": (c_int64, [c_void_p]),
         "reform_praq_destroy": (None, [c_void_p]),
         "reform_praq_bounds_noalloc": (I, [c_int64, c_int64, c_void_p, c_void_p, c_void_p,
@@ -120,6 +121,7 @@ def _declare(lib):
         "reform_pria_set_warm": (I, [c_void_p, D, D, D]),
         "reform_pria_result": (I, [c_void_p, D, D, D, P(PriaResultInfo)]),
         "reform_pria_run_profiled": (I, [c_void_p, D, P(c_int64)]),
+        "reform_pria_set_megakernel": (I, [c_void_p, c_int, P(c_int)]),
         "reform_pria_launches": (c_int64, [c_void_p]),
         "reform_pria_destroy": (None, [c_void_p]),
     })

@@ -408,6 +408,7 @@ struct Engine final : EngineBase {
         auto s = std::make_unique<praq::Solver<Real>>();
         s->p = p;
         s->allow_pull = false;   // the engine's kernels read slot 1 in the push layout
+        s->allow_mega = false;   // the engine runs its own kernels
         const int st = s->setup(in, lay);
         if (st) return st;
         if (joined(s->stream)) return PRAQ_ERROR_CUDA;

@@ -120,6 +120,79 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// ---- the grid barrier of a persistent (cooperative) launch -----------------
+// Every CTA arrives once per barrier; the last to arrive resets the count and
+// advances the generation the others wait on.  Waits are bounded: a CTA that
+// has waited `limit_ns` of %globaltimer, or that sees `err` set, sets `err`
+// and gives up, so a barrier that cannot complete ends the kernel with an
+// error the host reads (and clears before the next launch) instead of a hang.
+struct GridBar {
+    unsigned count, gen;
+    int err, pad;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// True when every one of `expect` CTAs has arrived; false when the wait ran
+// out or another CTA's did.  Memory written by any thread of any CTA before
+// the barrier is visible to every thread after it.
+__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned expect, unsigned long long limit_ns) {
+    if (expect == 1) {   // a grid of one CTA: the block barrier orders its global memory as well
+        __syncthreads();
+        return true;
+    }
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        const unsigned g = ld_acquire_gpu(&b->gen);
+        __threadfence();   // the CTA's writes, ordered by the barrier above, before the arrival
+        if (atom_add_acq_rel_gpu(&b->count, 1u) == expect - 1) {
+            atomicExch(&b->count, 0u);
+            st_release_gpu(&b->gen, g + 1);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            while (ld_acquire_gpu(&b->gen) == g) {
+                if (ld_relaxed_gpu(&b->err) || globaltimer_ns() - t0 > limit_ns) {
+                    atomicExch(&b->err, 1);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) {
     return v < lo ? lo : (v > hi ? hi : v);

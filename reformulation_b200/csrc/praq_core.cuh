@@ -148,9 +148,8 @@ constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 // (chunks of 4 loads per lane: 2 % faster per solve at n >= 1.5e5 than an
 // unrolled loop; 8 were no better).
 template <class Real, class Acc, bool Indexed>
-__device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* __restrict__ v,
-                                         const int* __restrict__ idx, int n, long long base, int lane,
-                                         Real* __restrict__ stage) {
+__device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* v, const int* __restrict__ idx,
+                                         int n, long long base, int lane, Real* __restrict__ stage) {
     if (base >= n) return Acc(0);   // uniform over the warp
     const long long i = base + lane;
     const long long last = base + 32 < n ? base + 32 : n;
@@ -216,9 +215,8 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
 // latency of a warp's dependent loads bounds.  All lanes of the warp must call
 // it with the same base.
 template <class Real, class Acc, bool IndexB>
-__device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Real* __restrict__ va,
-                                           const int* __restrict__ pb, const Real* __restrict__ vb,
-                                           const int* __restrict__ ib, int n, long long base, int lane,
+__device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Real* va, const int* __restrict__ pb,
+                                           const Real* vb, const int* __restrict__ ib, int n, long long base, int lane,
                                            Real* __restrict__ sa,
                                            Real* __restrict__ sb, Acc& ra, Acc& rb) {
     ra = Acc(0);
@@ -241,7 +239,7 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
         const int ea = min(ahi, ca + kStage), eb = min(bhi, cb + kStage);
         // lane-relative bases and counts, so each load is a base plus an
         // immediate offset
-        const Real* __restrict__ ga = va + (ca + lane);
+        const Real* ga = va + (ca + lane);
         const int na = ea - ca - lane, nb = eb - cb - lane;
         const int wide = max(ea - ca, eb - cb);   // the same on every lane
         if constexpr (IndexB) {
@@ -272,7 +270,7 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
                 if (32 * q < nb) sb[lane + 32 * q] = ta[q];
             }
         } else {
-            const Real* __restrict__ gb = vb + (cb + lane);
+            const Real* gb = vb + (cb + lane);
             Real ta[kPer], tb[kPer];
 #pragma unroll
             for (int q = 0; q < kPer; ++q) {
@@ -302,10 +300,19 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
 template <bool Wide>
 constexpr int stage_runs() { return Wide ? 2 : 1; }
 
+// This warp's staging slice: one shared buffer per precision and width for
+// every tile function of a kernel (the node step in its three forms and the
+// lower-bound pass share it in the persistent kernel), runs * stage_len
+// values per warp.
+template <class Real, int Runs>
+__device__ __forceinline__ Real* warp_stage() {
+    __shared__ Real stage[kBlock / 32][Runs * stage_len<Real>()];
+    return stage[threadIdx.x >> 5];
+}
+
 template <class Real, class Acc, bool Wide, bool Pull>
-__device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __restrict__ ys,
-                                          const Real* __restrict__ yc, long long base, int lane,
-                                          Real* __restrict__ stage) {
+__device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* ys, const Real* yc, long long base,
+                                          int lane, Real* __restrict__ stage) {
     if constexpr (Wide) {
         Acc s0, s1;
         warp_runs2<Real, Acc, Pull>(d.row_ptr, ys, d.col_ptr, yc, d.colidx, d.n, base, lane, stage,
@@ -323,12 +330,12 @@ __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* __rest
 // k = restart_iter + step + 1; vanilla: x1 = x2 and the anchor becomes x1.
 // Check: the node sums of this step go to pnode.
 template <class Real, bool Reflect, bool Check, bool Wide = false, bool Pull = false>
-__device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc, int step,
-            int bounds_at_1, int gate) {
+__device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, const Real* ys, const Real* yc, int step,
+                                                 int bounds_at_1, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
     __shared__ double scratch[kNodeSums * 32];
-    __shared__ Real stage[kBlock / 32][stage_runs<Wide>() * stage_len<Real>()];
+    Real* stage = warp_stage<Real, stage_runs<Wide>()>();
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
@@ -344,7 +351,7 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
             x0o = d.x0[i];
         }
     }
-    const Real s = scatter_at<Real, Real, Wide, Pull>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const Real s = scatter_at<Real, Real, Wide, Pull>(d, ys, yc, base, lane, stage);
     double acc[kNodeSums] = {0.0, 0.0, 0.0};
     if (owner) {
         Real x1v;
@@ -472,14 +479,14 @@ edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) 
 // The node part of the lower bound, sum_i min(d_i - (S^T y)_i, 0), at the
 // dual (ys, yc) (solver.py:333-337), in FP64.
 template <class Real, bool Wide = false, bool Pull = false>
-__device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ ys, const Real* __restrict__ yc) {
+__device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* ys, const Real* yc) {
     if (d.ctl->terminated) return;
     __shared__ double scratch[32];
-    __shared__ Real stage[kBlock / 32][stage_runs<Wide>() * stage_len<Real>()];
+    Real* stage = warp_stage<Real, stage_runs<Wide>()>();
     const int lane = threadIdx.x & 31;
     const long long base = (long long)tile * blockDim.x + (threadIdx.x & ~31);
     const long long i = base + lane;
-    const double s = scatter_at<Real, double, Wide, Pull>(d, ys, yc, base, lane, stage[threadIdx.x >> 5]);
+    const double s = scatter_at<Real, double, Wide, Pull>(d, ys, yc, base, lane, stage);
     double acc[1] = {0.0};
     if (i < d.n) {
         const double rc = double(d.diag[i]) - s;
@@ -512,9 +519,9 @@ __device__ __forceinline__ bool should_stop(double gap, long long iteration, con
 // mode 0: the check before the loop (bounds at (x1, y1));
 // mode 1: the check after an op_steps block (solver.py:397-469);
 // mode 2: after the restart step, the new fixed-point error.
-__device__ __forceinline__ void check_body(Control* c, Params p, const double* __restrict__ scale_ptr,
-             const double* __restrict__ pnode, int nbn, const double* __restrict__ pedge, int nbe,
-             const double* __restrict__ plower, int nbl, int mode) {
+__device__ __forceinline__ void check_body(Control* c, Params p, const double* scale_ptr, const double* pnode,
+                                           int nbn, const double* pedge, int nbe, const double* plower, int nbl,
+                                           int mode) {
     if (c->terminated) return;
     if (mode == 2 && !c->restart) return;
     __shared__ double scratch[kEdgeSums * 32];
@@ -581,6 +588,88 @@ check_kernel(Control* c, Params p, const double* __restrict__ scale_ptr,
     pdl_wait();
     pdl_launch_dependents();
     check_body(c, p, scale_ptr, pnode, nbn, pedge, nbe, plower, nbl, mode);
+}
+
+// ---- the persistent kernel for small instances ----------------------------
+// One cooperative launch runs a whole check block: op_steps steps of the node
+// half and the edge half, the lower-bound pass, the check and the gated
+// restart step -- the graph's tile functions in the graph's order with the
+// graph's CTA shape, so the results are the graph's bit for bit -- each
+// phase's tiles dealt round-robin to the resident CTAs and the phases
+// separated by grid barriers (bounded waits, common.cuh; a grid of one CTA,
+// as for a few hundred nodes, needs only block barriers).  For instances of a
+// few thousand edges a kernel boundary costs more than the phase it ends.  The
+// tile functions take the iterates through plain pointers (no __restrict__):
+// here a buffer one phase reads, another phase of the same launch writes.  A
+// barrier that runs out sets Control::status to kMegaWaitStatus.
+constexpr int kMegaWaitStatus = 1;
+
+struct MegaArgs {
+    GridBar* bar;
+    unsigned expect;                 // CTAs each barrier waits for (the grid)
+    unsigned long long wait_ns;      // a barrier's wait limit
+    int nb_node, nb_edge;            // tiles of the node and edge halves
+};
+
+template <class Real, bool Reflect, bool Check, bool Wide>
+__device__ __forceinline__ void mega_node(const Dev<Real>& d, const MegaArgs& a, const Real* ys, const Real* yc,
+                                          int step, int gate) {
+    for (int t = int(blockIdx.x); t < a.nb_node; t += gridDim.x) {
+        node_kernel_tile<Real, Reflect, Check, Wide, false>(d, t, ys, yc, step, 0, gate);
+        __syncthreads();   // the next tile reuses the staging buffer
+    }
+}
+
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void mega_edge(const Dev<Real>& d, const MegaArgs& a, const Real* ysrc, int step,
+                                          int gate) {
+    for (int t = int(blockIdx.x); t < a.nb_edge; t += gridDim.x) {
+        edge_kernel_tile<Real, Reflect, Check, false>(d, t, ysrc, step, 0, gate);
+        __syncthreads();
+    }
+}
+
+// The push layout only (the slot-1 pull layout is for edge arrays beyond L2).
+template <class Real, bool Wide>
+__global__ void __launch_bounds__(kBlock, 1)
+mega_block_kernel(const __grid_constant__ Dev<Real> d, const __grid_constant__ Params prm, MegaArgs a) {
+    const int op = int(prm.op_steps);
+    auto sync = [&]() {
+        if (grid_sync(a.bar, a.expect, a.wait_ns)) return true;
+        if (threadIdx.x == 0) d.ctl->status = kMegaWaitStatus;
+        return false;
+    };
+    for (int s = 0; s < op; ++s) {
+        if (s + 1 < op)
+            mega_node<Real, true, false, Wide>(d, a, d.pred, d.pred1, s, 0);
+        else
+            mega_node<Real, true, true, Wide>(d, a, d.pred, d.pred1, s, 0);
+        if (!sync()) return;
+        if (d.m) {
+            if (s + 1 < op)
+                mega_edge<Real, true, false>(d, a, nullptr, s, 0);
+            else
+                mega_edge<Real, true, true>(d, a, nullptr, s, 0);
+            if (!sync()) return;
+        }
+    }
+    for (int t = int(blockIdx.x); t < a.nb_node; t += gridDim.x) {
+        lower_kernel_tile<Real, Wide, false>(d, t, d.u2s, d.u2s1);
+        __syncthreads();
+    }
+    if (!sync()) return;
+    if (blockIdx.x == 0)
+        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 1);
+    if (!sync()) return;
+    if (!d.ctl->restart) return;   // uniform: the check above is the last writer
+    mega_node<Real, false, true, Wide>(d, a, d.u2s, d.u2s1, 0, 1);
+    if (!sync()) return;
+    if (d.m) {
+        mega_edge<Real, false, true>(d, a, d.u2s, 0, 1);
+        if (!sync()) return;
+    }
+    if (blockIdx.x == 0)
+        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 2);
 }
 
 // Cold start: the centroid, x = 1/2 and y_e = (-W_ij, -W_ij) / scale, which is
@@ -770,6 +859,9 @@ struct SolverBase {
     virtual int result(double* x, double* y2, PraqResult* r) = 0;
     virtual long long launches() const = 0;
     virtual int run_profiled(double* ms, long long* count) = 0;
+    // -1 auto, 0 the graph, 1 the persistent kernel where the instance allows
+    // it; *active: which one later runs take
+    virtual int set_megakernel(int mode, int* active) = 0;
     double time_limit = -1.0;   // seconds of wall clock per run; < 0: none
 };
 
@@ -792,12 +884,23 @@ struct Solver final : SolverBase {
     bool wide = false;   // node gather of both runs at once (warp_runs2)
     bool pull = false;   // slot-1 layout (see the layout notes at the top)
     bool allow_pull = true;   // false: always push (the batched engine's kernels)
+    bool allow_mega = true;   // false: never the persistent kernel (the batched engine's instances)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
     int status_override = -100;
     int runs = 0;
+    // The persistent kernel (mega_block_kernel) in place of the graph: chosen
+    // at set-up (mode -1: when a step's arrays take at most kMegaAutoBytes), or
+    // forced by set_mega; mega_grid resident CTAs.
+    bool mega = false;
+    int mega_mode = -1;              // -1 auto, 0 off, 1 on where the instance allows it
+    int mega_grid = 0;
+    unsigned mega_phantom = 0;       // CTAs the barriers also wait for, never launched (fault injection)
+    unsigned long long mega_wait_ns = 1000000000ull;
+    PoolBuf<GridBar> bar;
+    static constexpr long long kMegaAutoBytes = 2LL << 20;
 
     ~Solver() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -810,7 +913,7 @@ struct Solver final : SolverBase {
         w.release(); diag.release(); deg.release();
         x1.release(); x2.release(); x0.release(); r.release(); pred.release(); pred1.release();
         u0.release(); u2s.release(); u2s1.release();
-        pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release();
+        pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release(); bar.release();
         warm_x.release(); warm_y.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
@@ -878,8 +981,76 @@ struct Solver final : SolverBase {
         prm.theta_target = p.theta_target;
         prm.theta_decay = p.theta_decay;
         block_nodes = (m ? 2 : 1) * (long long)p.op_steps + 2 + (m ? 2 : 1) + 1;
+        if (init_mega() != cudaSuccess) return PRAQ_ERROR_CUDA;
         return cudaGetLastError() == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
     }
+
+    // --- the persistent kernel -------------------------------------------
+    // Bytes a step streams: per edge ends, weight, colpos and four reals
+    // (w, pred, pred1, u0), per node the run pointers and seven reals.
+    long long step_bytes() const {
+        return (long long)m * (12 + 4 * (long long)sizeof(Real)) + (long long)n * (8 + 7 * (long long)sizeof(Real));
+    }
+
+    cudaError_t init_mega() {
+        mega_grid = 0;
+        if (!allow_mega) return cudaSuccess;
+        if (!pull) {
+            int dev = 0, sms = 0, per_sm = 0;
+            auto fn = wide ? mega_block_kernel<Real, true> : mega_block_kernel<Real, false>;
+            RB_CUDA_TRY(cudaGetDevice(&dev));
+            RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+            // no phase has more tiles than this: more CTAs would only wait
+            mega_grid = int(std::min<long long>((long long)per_sm * sms, std::max(nb_node, m ? nb_edge : 1)));
+        }
+        // REFORM_PRAQ_MEGA=0|1 sets the initial mode (tests, measurements);
+        // REFORM_PRAQ_MEGA_PHANTOM=k makes every barrier wait for k CTAs that
+        // are never launched, so each wait runs out (the fault-injection test)
+        const char* env = std::getenv("REFORM_PRAQ_MEGA");
+        int mode = -1;
+        if (env && (env[0] == '0' || env[0] == '1') && env[1] == '\0') mode = env[0] - '0';
+        const char* ph = std::getenv("REFORM_PRAQ_MEGA_PHANTOM");
+        if (ph) {
+            mega_phantom = unsigned(std::strtoul(ph, nullptr, 10));
+            if (mega_phantom) mega_wait_ns = 50000000ull;   // 50 ms: the test waits for every barrier
+        }
+        return set_mega(mode);
+    }
+
+    cudaError_t set_mega(int mode) {
+        mega_mode = mode < 0 ? -1 : (mode ? 1 : 0);
+        const bool want = mega_mode == 1 || (mega_mode < 0 && step_bytes() <= kMegaAutoBytes);
+        mega = want && mega_grid > 0;
+        if (mega && !bar.ptr) {
+            RB_CUDA_TRY(bar.alloc(1, stream));
+            RB_CUDA_TRY(cudaMemsetAsync(bar.ptr, 0, sizeof(GridBar), stream));
+        }
+        return cudaSuccess;
+    }
+
+    int set_megakernel(int mode, int* active) override {
+        const cudaError_t st = set_mega(mode);
+        if (active) *active = mega ? 1 : 0;
+        return st == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
+    }
+
+    cudaError_t launch_mega() {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(mega_grid));
+        cfg.blockDim = dim3(unsigned(kBlock));
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;   // every CTA resident at once, or no launch
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const MegaArgs a{bar.ptr, unsigned(mega_grid) + mega_phantom, mega_wait_ns, nb_node, nb_edge};
+        if (wide) return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, true>, d, prm, a);
+        return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, false>, d, prm, a);
+    }
+    long long block_launches() const { return mega ? 1 : block_nodes; }
 
     int layout(const PraqInstance& in) {
         n = int(in.n);
@@ -949,7 +1120,7 @@ struct Solver final : SolverBase {
     }
 
     // --- profiling: an event pair around every kernel, by kind ------------
-    static constexpr int kKinds = 9;
+    static constexpr int kKinds = 10;   // the graph's nine kinds; a persistent-kernel block
     std::vector<cudaEvent_t> evpool;
     std::vector<std::pair<int, int>> marks;   // (kind, first event index)
     bool profiling = false;
@@ -981,6 +1152,10 @@ struct Solver final : SolverBase {
     // sums), the lower-bound pass, the check, then the restart step (gated on
     // the device flag), its error, and a copy of the control block to the host.
     cudaError_t enqueue_block() {
+        if (mega) {
+            RB_TIMED(9, RB_CUDA_TRY(launch_mega()));
+            return cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+        }
         if (pull) return wide ? enqueue_steps<true, true>() : enqueue_steps<false, true>();
         return wide ? enqueue_steps<true, false>() : enqueue_steps<false, false>();
     }
@@ -1017,7 +1192,7 @@ struct Solver final : SolverBase {
         return cudaGraphInstantiate(&exec, graph, 0);
     }
 
-    cudaError_t launch_block() { return exec ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
+    cudaError_t launch_block() { return exec && !mega ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
 
     // The start point of later runs: x [n] and dual pairs y2 [2m] (instance
     // units, the input's edge order, as result() returns them); either may be
@@ -1070,6 +1245,7 @@ struct Solver final : SolverBase {
     // Cold (or warm) start, the first vanilla step and the check before the loop.
     int start_solve() {
         nlaunch = 0;
+        if (mega && cudaMemsetAsync(bar.ptr, 0, sizeof(GridBar), stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
         const int count = std::max(n, m);
         if (warm_x.ptr || warm_y.ptr)
             warm_init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(
@@ -1094,7 +1270,7 @@ struct Solver final : SolverBase {
         const auto started = std::chrono::steady_clock::now();
         bool timed_out = false;
         // the first run launches directly; repeated runs replay a captured block
-        if (runs++ > 0 && !exec && capture_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
+        if (runs++ > 0 && !exec && !mega && capture_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
         {
             const int st = start_solve();
             if (st) return st;
@@ -1105,12 +1281,12 @@ struct Solver final : SolverBase {
             for (int k = 0; k < 2; ++k) {
                 if (launch_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
                 if (cudaEventRecord(done[k], stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                nlaunch += block_nodes;
+                nlaunch += block_launches();
             }
             int k = 0;
             for (;;) {
                 if (cudaEventSynchronize(done[k]) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                if (mirror->terminated) break;
+                if (mirror->status || mirror->terminated) break;
                 if (time_limit >= 0.0 &&
                     std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() >
                         time_limit) {
@@ -1119,13 +1295,14 @@ struct Solver final : SolverBase {
                 }
                 if (launch_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
                 if (cudaEventRecord(done[k], stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
-                nlaunch += block_nodes;
+                nlaunch += block_launches();
                 k ^= 1;
             }
         }
         if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
             cudaStreamSynchronize(stream) != cudaSuccess)
             return PRAQ_ERROR_CUDA;
+        if (mirror->status) return PRAQ_ERROR_CUDA;   // a barrier of the persistent kernel ran out
         if (timed_out && !mirror->terminated) {
             mirror->result_slot = 2;
             status_override = PRAQ_STATUS_TIME_LIMIT;
@@ -1150,7 +1327,11 @@ struct Solver final : SolverBase {
                 profiling = false;
                 return PRAQ_ERROR_CUDA;
             }
-            nlaunch += block_nodes;
+            nlaunch += block_launches();
+            if (mirror->status) {
+                profiling = false;
+                return PRAQ_ERROR_CUDA;
+            }
             for (auto& mk : marks) {
                 float t = 0.f;
                 if (cudaEventElapsedTime(&t, evpool[mk.second], evpool[mk.second + 1]) != cudaSuccess) {

@@ -92,10 +92,15 @@ int reform_praq_set_time_limit(reform_praq_solver* solver, double seconds) {
 
 int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* count) {
     if (!solver || !solver->impl || !ms || !count) return PRAQ_ERROR_ARGUMENT;
-    long long c[9];
+    long long c[10];
     const int st = solver->impl->run_profiled(ms, c);
-    for (int k = 0; k < 9; ++k) count[k] = c[k];
+    for (int k = 0; k < 10; ++k) count[k] = c[k];
     return st;
+}
+
+int reform_praq_set_megakernel(reform_praq_solver* solver, int mode, int* active) {
+    if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
+    return solver->impl->set_megakernel(mode, active);
 }
 
 int64_t reform_praq_launches(const reform_praq_solver* solver) {

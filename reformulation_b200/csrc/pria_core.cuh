@@ -257,7 +257,7 @@ __device__ double michelot_smem(const Real* v, int len, double target, double wa
 // vanilla: xsrc is the point itself and becomes the anchor.  Check: x2 and
 // x1 - x2 are kept and the x sums go to px.
 template <class Real, int TW, bool Reflect, bool Check>
-__device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, const Real* xsrc, const Real* __restrict__ ysrc, const Real* __restrict__ zsrc,
+__device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, const Real* xsrc, const Real* ysrc, const Real* zsrc,
          int step, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
@@ -534,6 +534,25 @@ struct MichelotSteps {
     }
 };
 
+// The CTAs that share one z task: the CTAs of a cluster (ZGroup<false>), or
+// one CTA alone (ZGroup<true>, the persistent kernel, whose launch has no
+// clusters), with the same interface so that z_task's arithmetic is one code.
+template <bool Solo>
+struct ZGroup {
+    cg::cluster_group g = cg::this_cluster();
+    __device__ __forceinline__ int rank() const { return int(g.block_rank()); }
+    __device__ __forceinline__ void sync() { g.sync(); }
+    template <class T>
+    __device__ __forceinline__ T* peer(T* p, int r) { return g.map_shared_rank(p, r); }
+};
+template <>
+struct ZGroup<true> {
+    __device__ __forceinline__ int rank() const { return 0; }
+    __device__ __forceinline__ void sync() { __syncthreads(); }
+    template <class T>
+    __device__ __forceinline__ T* peer(T* p, int) { return p; }
+};
+
 // Sums of K values over every thread of every CTA of a cluster, bitwise the
 // same on every CTA, with one cluster barrier: each warp's total goes to its
 // slot of slots[parity]; after the barrier warp 0 of each CTA adds all ranks'
@@ -541,10 +560,9 @@ struct MichelotSteps {
 // same on every CTA) and one CTA barrier hands the totals to every thread.
 // A round may reuse slots[parity] two rounds later: the barrier of the round
 // between them is reached by every warp 0 only after its reads.
-template <int K, int kWarps>
+template <int K, int kWarps, class Group>
 __device__ __forceinline__ void cluster_sums(const double (&v)[K], double (*slots)[kWarps][K], double* tot,
-                                             int parity, cg::cluster_group& cluster, int csize,
-                                             double (&out)[K]) {
+                                             int parity, Group& cluster, int csize, double (&out)[K]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -557,7 +575,7 @@ __device__ __forceinline__ void cluster_sums(const double (&v)[K], double (*slot
 #pragma unroll
         for (int k = 0; k < K; ++k) a[k] = 0.0;
         for (int idx = lane; idx < csize * kWarps; idx += 32) {
-            const double* pp = cluster.map_shared_rank(&slots[parity][idx % kWarps][0], idx / kWarps);
+            const double* pp = cluster.peer(&slots[parity][idx % kWarps][0], idx / kWarps);
 #pragma unroll
             for (int k = 0; k < K; ++k) a[k] += pp[k];
         }
@@ -576,14 +594,16 @@ __device__ __forceinline__ void cluster_sums(const double (&v)[K], double (*slot
 // per block; CTA `rank` owns rows [r0, r1) of the block, a contiguous slice.
 // z + r of the slice goes to shared memory, the threshold of the whole block
 // comes from Michelot rounds whose (sum, count) pass through distributed
-// shared memory, then the slice's z is written.
-template <class Real, int kThreads, bool Reflect, bool Check>
+// shared memory, then the slice's z is written.  Solo: the whole block in
+// this CTA (csize 1), CTA barriers in place of cluster barriers, the same
+// sums in the same order.
+template <class Real, int kThreads, bool Reflect, bool Check, bool Solo = false>
 __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zsrc, int step, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
-    cg::cluster_group cluster = cg::this_cluster();
-    const int csize = d.csize;
-    const int rank = int(cluster.block_rank());
+    ZGroup<Solo> cluster;
+    const int csize = Solo ? 1 : d.csize;
+    const int rank = cluster.rank();
     const int len = d.tp - s;
     const long long base = blk(d.n, d.tp, s);
     const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
@@ -704,9 +724,9 @@ template <class Real, int kThreads, bool Reflect, bool Check>
 __device__ __forceinline__ void z_task_pair(const Dev<Real>& d, int pair, const Real* zsrc, int step, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;   // uniform over the cluster: c is not written here
-    cg::cluster_group cluster = cg::this_cluster();
+    ZGroup<false> cluster;
     const int csize = d.csize;
-    const int rank = int(cluster.block_rank());
+    const int rank = cluster.rank();
     const int r0 = int((long long)d.n * rank / csize), r1 = int((long long)d.n * (rank + 1) / csize);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real* vz = reinterpret_cast<Real*>(smem_raw);
@@ -875,7 +895,7 @@ constexpr auto z_entry() {
 // block, restricted to t < tlimit and s < tlimit (tlimit = t for the unpadded
 // objective).  `force` runs it after termination.
 template <class Real>
-__device__ __forceinline__ void upper_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ x, int tlimit, int force) {
+__device__ __forceinline__ void upper_kernel_tile(const Dev<Real>& d, int tile, const Real* x, int tlimit, int force) {
     if (!force && d.ctl->terminated) return;
     __shared__ double scratch[3 * 32];
     __shared__ double wmax[32];
@@ -939,7 +959,7 @@ upper_kernel(Dev<Real> d, const Real* __restrict__ x, int tlimit, int force) {
 // The dual bound sum_{i,t} min_{s<=t} (h + y + z) (solver.py:388-402) for one
 // tile of kLowTW columns of one item.
 template <class Real>
-__device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* __restrict__ y, const Real* __restrict__ z) {
+__device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, const Real* y, const Real* z) {
     if (d.ctl->terminated) return;
     __shared__ double cmin[kAuxThreads / 32][kLowTW];
     __shared__ double scratch[32];
@@ -1004,9 +1024,9 @@ __device__ __forceinline__ bool should_stop(double gap, long long iteration, con
 // bounds at the current point, solver.py:601-606); 4: after the step that
 // ends the vanilla phase and starts the Halpern one (the primal weight from
 // the drift of the vanilla phase, solver.py:680-694).
-__device__ __forceinline__ void check_body(Control* c, Params p, const double* __restrict__ px, int nbx,
-             const double* __restrict__ py, int nby, const double* __restrict__ pyz, int nbyz,
-             const double* __restrict__ pup, int nbup, const double* __restrict__ plo, int nblo, int mode) {
+__device__ __forceinline__ void check_body(Control* c, Params p, const double* px, int nbx, const double* py,
+                                           int nby, const double* pyz, int nbyz, const double* pup, int nbup,
+                                           const double* plo, int nblo, int mode) {
     if (c->terminated) return;
     if (mode == 2 && !c->restart) return;
     __shared__ double scratch[3 * 32];
@@ -1116,6 +1136,131 @@ check_kernel(Control* c, Params p, const double* __restrict__ px, int nbx,
              const double* __restrict__ pyz, int nbyz, const double* __restrict__ pup, int nbup,
              const double* __restrict__ plo, int nblo, int mode) {
     check_body(c, p, px, nbx, py, nby, pyz, nbyz, pup, nbup, plo, nblo, mode);
+}
+
+// ---- the persistent kernel for small instances ----------------------------
+// (the reference's megakernel, jrp/pria-cuda/src/solver.cuh:145-312, on this
+// file's own half-steps.)  One cooperative launch runs a whole check block:
+// op_steps steps of x, then y and z, the bounds, the check and the gated
+// restart step, the same tile functions as the per-kernel graph in the same
+// order, each phase's units dealt round-robin to the resident CTAs and the
+// phases separated by grid barriers (bounded waits, common.cuh).  It replaces
+// the graph's 55 kernel boundaries per block by 34 barriers (37 with a
+// restart).  A z task is one whole period block in one CTA (ZGroup<true>), so
+// instances whose largest block does not fit one CTA's shared memory keep the
+// graph.  The tile functions take their iterates through plain pointers (no
+// __restrict__): here a buffer one phase reads, another phase of the same
+// launch writes, and only the per-kernel wrappers may promise read-only data.
+// A barrier that runs out sets Control::status to kMegaWaitStatus.
+constexpr int kMegaThreads = 256;   // = kXThreads = kYThreads = kAuxThreads = kCheckBlock
+constexpr int kMegaWaitStatus = 1;
+#ifndef RB200_PRIA_MEGA_MINB
+#define RB200_PRIA_MEGA_MINB 1          // CTAs per SM the kernel is compiled for (sweeps build with -D)
+#endif
+
+struct MegaArgs {
+    GridBar* bar;
+    unsigned expect;                 // CTAs each barrier waits for (the grid)
+    unsigned long long wait_ns;      // a barrier's wait limit
+};
+
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void mega_x(const Dev<Real>& d, const Real* xs, const Real* ys, const Real* zs, int step,
+                                       int gate) {
+    const int tiles = d.n * d.ntc;
+    for (int tile = int(blockIdx.x); tile < tiles; tile += gridDim.x) {
+        x_kernel_tile<Real, kXTile, Reflect, Check>(d, tile, xs, ys, zs, step, gate);
+        __syncthreads();   // the next tile reuses the shared tile
+    }
+}
+
+// Out of line: inlined into the step loop, the z task's register demand grows
+// past the budget of the whole kernel.
+template <class Real, bool Reflect, bool Check>
+__device__ __noinline__ void mega_z(const Dev<Real>& d, int s, const Real* zs, int step, int gate) {
+    z_task<Real, kMegaThreads, Reflect, Check, true>(d, s, zs, step, gate);
+}
+
+// The z tasks (heaviest first) and then the y tiles of one half-step.
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void mega_yz(const Dev<Real>& d, const Real* ys, const Real* zs, int step, int gate) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nby = int(((long long)d.tp * d.n + kYThreads / 32 - 1) / (kYThreads / 32));
+    const int units = d.tp + nby;
+    for (int u = int(blockIdx.x); u < units; u += gridDim.x) {
+        if (u < d.tp)
+            mega_z<Real, Reflect, Check>(d, u, zs, step, gate);
+        else
+            y_kernel_tile<Real, Reflect, Check>(d, u - d.tp, ys, step, gate, reinterpret_cast<Real*>(smem_raw), d.tp);
+        __syncthreads();
+    }
+}
+
+template <class Real>
+__device__ __forceinline__ void mega_bounds(const Dev<Real>& d, const Real* x, const Real* y, const Real* z) {
+    const int units = d.tp + d.n * d.ntc_low;
+    for (int u = int(blockIdx.x); u < units; u += gridDim.x) {
+        if (u < d.tp)
+            upper_kernel_tile<Real>(d, u, x, d.tp, 0);
+        else
+            lower_kernel_tile<Real>(d, u - d.tp, y, z);
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void mega_check(Control* c, const Params& prm, const double* px, int nbx, const double* py,
+                                           int nby, const double* pyz, int nbyz, const double* pup, int nbup,
+                                           const double* plo, int nblo, int mode) {
+    if (blockIdx.x == 0) check_body(c, prm, px, nbx, py, nby, pyz, nbyz, pup, nbup, plo, nblo, mode);
+}
+
+// Vanilla: one block of the vanilla phase (enqueue_vanilla_block's steps);
+// otherwise one Halpern check block (enqueue_block's).
+template <class Real, bool Vanilla>
+__global__ void __launch_bounds__(kMegaThreads, RB200_PRIA_MEGA_MINB)
+mega_block_kernel(const __grid_constant__ Dev<Real> d, const __grid_constant__ Params prm, MegaArgs a) {
+    const int op = int(prm.op_steps);
+    const int nbx = d.n * d.ntc, nblo = d.n * d.ntc_low;
+    const int nby = int(((long long)d.tp * d.n + kYThreads / 32 - 1) / (kYThreads / 32));
+    auto sync = [&]() {
+        if (grid_sync(a.bar, a.expect, a.wait_ns)) return true;
+        if (threadIdx.x == 0) d.ctl->status = kMegaWaitStatus;
+        return false;
+    };
+    if constexpr (Vanilla) {
+        for (int s = 0; s < op; ++s) {
+            mega_x<Real, false, false>(d, d.xh, d.yh, d.zh, 0, kGateVanilla);
+            if (!sync()) return;
+            mega_yz<Real, false, false>(d, d.yh, d.zh, 0, kGateVanilla);
+            if (!sync()) return;
+        }
+        mega_bounds<Real>(d, d.xh, d.yh, d.zh);
+        if (!sync()) return;
+        mega_check(d.ctl, prm, d.px, nbx, d.py, nby, d.pyz, d.tp, d.pup, d.tp, d.plo, nblo, 3);
+    } else {
+        for (int s = 0; s < op; ++s) {
+            if (s + 1 < op)
+                mega_x<Real, true, false>(d, d.xh, d.yh, d.zh, s, 0);
+            else
+                mega_x<Real, true, true>(d, d.xh, d.yh, d.zh, s, 0);
+            if (!sync()) return;
+            if (s + 1 < op)
+                mega_yz<Real, true, false>(d, d.yh, d.zh, s, 0);
+            else
+                mega_yz<Real, true, true>(d, d.yh, d.zh, s, 0);
+            if (!sync()) return;
+        }
+        mega_bounds<Real>(d, d.x2s, d.y2s, d.z2s);
+        if (!sync()) return;
+        mega_check(d.ctl, prm, d.px, nbx, d.py, nby, d.pyz, d.tp, d.pup, d.tp, d.plo, nblo, 1);
+        if (!sync()) return;
+        if (!d.ctl->restart) return;   // uniform: the check above is the last writer
+        mega_x<Real, false, true>(d, d.x2s, d.y2s, d.z2s, 0, kGateRestart);
+        if (!sync()) return;
+        mega_yz<Real, false, true>(d, d.y2s, d.z2s, 0, kGateRestart);
+        if (!sync()) return;
+        mega_check(d.ctl, prm, d.px, nbx, d.py, nby, d.pyz, d.tp, d.pup, d.tp, d.plo, nblo, 2);
+    }
 }
 
 // The start point: the projection of zero, i.e. each simplex's centre:
@@ -1364,6 +1509,9 @@ struct SolverBase {
     virtual int set_warm(const double* wx, const double* wy, const double* wz) = 0;
     virtual long long launches() const = 0;
     virtual int run_profiled(double* ms, long long* count) = 0;
+    // -1 auto, 0 the graph, 1 the persistent kernel where the instance allows
+    // it; *active: which one later runs take
+    virtual int set_megakernel(int mode, int* active) = 0;
 };
 
 template <class Real>
@@ -1388,6 +1536,18 @@ struct Solver final : SolverBase {
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
     int runs = 0;
+    // The persistent kernel (mega_block_kernel) in place of the graph: chosen
+    // at set-up (mode -1: at most kMegaAutoEntries packed entries), or forced
+    // by set_mega; mega_grid resident CTAs of mega_smem bytes each.
+    bool mega = false;
+    int mega_mode = -1;              // -1 auto, 0 off, 1 on where the instance allows it
+    int mega_grid = 0;
+    size_t mega_smem = 0;
+    unsigned mega_phantom = 0;       // CTAs the barriers also wait for, never launched (fault injection)
+    unsigned long long mega_wait_ns = 1000000000ull;
+    PoolBuf<GridBar> bar;
+    static constexpr size_t kMegaSmemLimit = 96 * 1024;
+    static constexpr long long kMegaAutoEntries = 16384;
     static constexpr int kZThreadsPerCta = z_threads<Real>();
     // y rows: one padded row of at most kMaxPeriods reals per warp
     static constexpr size_t y_smem_limit() { return size_t(kYThreads / 32) * kMaxPeriods * sizeof(Real); }
@@ -1408,6 +1568,7 @@ struct Solver final : SolverBase {
         for (auto* b : {&h, &k, &xh, &x0, &r, &yh, &y0, &zh, &z0, &x2s, &dxs, &y2s, &z2s}) b->release();
         for (auto* b : {&px, &py, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
         for (auto& b : warm) b.release();
+        bar.release();
         ctl.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
@@ -1578,7 +1739,75 @@ struct Solver final : SolverBase {
         prm.vanilla_solve = p.use_halpern ? 0 : 1;
         RB_CUDA_TRY(set_attributes());
         block_nodes = 3LL * p.op_steps + 3 + 4;   // x, y, z per step; bounds, check; restart x, y, z, check
+        RB_CUDA_TRY(init_mega());
         return cudaGetLastError();
+    }
+
+    // --- the persistent kernel -------------------------------------------
+    // It needs every z task in one CTA (cluster size 1, single blocks, staged
+    // in shared memory) and its dynamic shared memory (the largest of the x
+    // tile, the y rows, the z block) within kMegaSmemLimit.
+    bool mega_possible() const {
+        return mega_grid > 0 && d.csize == 1 && !d.zpair && d.zstaged && mega_smem <= kMegaSmemLimit;
+    }
+
+    cudaError_t init_mega() {
+        mega_smem = std::max({x_smem, size_t(kYThreads / 32) * tp * sizeof(Real), yz_smem});
+        mega_grid = 0;
+        if (mega_smem <= kMegaSmemLimit) {
+            int dev = 0, sms = 0, per_sm = 1 << 30;
+            RB_CUDA_TRY(cudaGetDevice(&dev));
+            RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            for (auto fn : {mega_block_kernel<Real, false>, mega_block_kernel<Real, true>}) {
+                int k = 0;
+                RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(kMegaSmemLimit)));
+                RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, fn, kMegaThreads, mega_smem));
+                per_sm = std::min(per_sm, k);
+            }
+            // no phase has more units than this: more CTAs would only wait
+            const long long units = std::max({(long long)nbx, (long long)tp + nby, (long long)tp + nblo});
+            mega_grid = int(std::min<long long>((long long)per_sm * sms, units));
+        }
+        // REFORM_PRIA_MEGA=0|1 sets the initial mode (tests, measurements);
+        // REFORM_PRIA_MEGA_PHANTOM=k makes every barrier wait for k CTAs that
+        // are never launched, so each wait runs out (the fault-injection test)
+        const char* env = std::getenv("REFORM_PRIA_MEGA");
+        int mode = -1;
+        if (env && (env[0] == '0' || env[0] == '1') && env[1] == '\0') mode = env[0] - '0';
+        const char* ph = std::getenv("REFORM_PRIA_MEGA_PHANTOM");
+        if (ph) {
+            mega_phantom = unsigned(std::strtoul(ph, nullptr, 10));
+            if (mega_phantom) mega_wait_ns = 50000000ull;   // 50 ms: the test waits for every barrier
+        }
+        return set_mega(mode);
+    }
+
+    cudaError_t set_mega(int mode) {
+        mega_mode = mode < 0 ? -1 : (mode ? 1 : 0);
+        const bool want = mega_mode == 1 || (mega_mode < 0 && nd <= kMegaAutoEntries);
+        mega = want && mega_possible();
+        if (mega && !bar.ptr) {
+            RB_CUDA_TRY(bar.alloc(1, stream));
+            RB_CUDA_TRY(cudaMemsetAsync(bar.ptr, 0, sizeof(GridBar), stream));
+        }
+        return cudaSuccess;
+    }
+
+    cudaError_t launch_mega(bool vanilla) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(mega_grid));
+        cfg.blockDim = dim3(unsigned(kMegaThreads));
+        cfg.dynamicSmemBytes = mega_smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;   // every CTA resident at once, or no launch
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const MegaArgs a{bar.ptr, unsigned(mega_grid) + mega_phantom, mega_wait_ns};
+        if (vanilla) return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, true>, d, prm, a);
+        return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, false>, d, prm, a);
     }
 
     // The dynamic shared-memory limit is a property of the kernel, shared by
@@ -1659,7 +1888,7 @@ struct Solver final : SolverBase {
     }
 
     // --- profiling ------------------------------------------------------
-    static constexpr int kKinds = 8;
+    static constexpr int kKinds = 9;   // x, yz, x and yz at the check, upper, lower, check, restart; a mega block
     std::vector<cudaEvent_t> evpool;
     std::vector<std::pair<int, int>> marks;
     bool profiling = false;
@@ -1686,6 +1915,10 @@ struct Solver final : SolverBase {
     } while (0)
 
     cudaError_t enqueue_block() {
+        if (mega) {
+            RB_PTIMED(8, launch_mega(false));
+            return cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+        }
         const int op = p.op_steps;
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
@@ -1715,7 +1948,16 @@ struct Solver final : SolverBase {
         return cudaGraphInstantiate(&exec, graph, 0);
     }
 
-    cudaError_t launch_block() { return exec ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
+    cudaError_t launch_block() { return exec && !mega ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
+    long long block_launches() const { return mega ? 1 : block_nodes; }
+    // the error of a block whose grid barrier ran out (the persistent kernel)
+    static constexpr int kMegaWaitError = int(cudaErrorLaunchTimeout);
+
+    int set_megakernel(int mode, int* active) override {
+        const cudaError_t st = set_mega(mode);
+        if (active) *active = mega ? 1 : 0;
+        return int(st);
+    }
 
     int set_warm(const double* wx, const double* wy, const double* wz) override {
         if (!wx || !wy || !wz) {
@@ -1732,6 +1974,7 @@ struct Solver final : SolverBase {
 
     cudaError_t start_solve() {
         nlaunch = 0;
+        if (mega) RB_CUDA_TRY(cudaMemsetAsync(bar.ptr, 0, sizeof(GridBar), stream));
         // every run starts its thresholds cold (all-NaN bytes)
         RB_CUDA_TRY(cudaMemsetAsync(thx.ptr, 0xFF, sizeof(double) * thx.count, stream));
         RB_CUDA_TRY(cudaMemsetAsync(thy.ptr, 0xFF, sizeof(double) * thy.count, stream));
@@ -1761,6 +2004,11 @@ struct Solver final : SolverBase {
     // One check block of the vanilla phase: op_steps plain steps of the
     // current point in place, then the bounds at it and the check (mode 3).
     cudaError_t enqueue_vanilla_block() {
+        if (mega) {
+            RB_CUDA_TRY(launch_mega(true));
+            nlaunch += 1;
+            return cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+        }
         for (int s = 0; s < p.op_steps; ++s) {
             RB_CUDA_TRY((launch_x<false, false>(d.xh, d.yh, d.zh, 0, kGateVanilla)));
             RB_CUDA_TRY((launch_yz<false, false>(d.yh, d.zh, 0, kGateVanilla)));
@@ -1789,6 +2037,7 @@ struct Solver final : SolverBase {
         for (;;) {
             RB_CUDA_TRY(enqueue_vanilla_block());
             RB_CUDA_TRY(cudaStreamSynchronize(stream));
+            if (mirror->status) return cudaErrorLaunchTimeout;
             if (mirror->terminated || mirror->phase_done) break;
             if (over_budget(started)) {
                 timed_out = true;        // the last check's point: the current one (slot 3)
@@ -1810,7 +2059,8 @@ struct Solver final : SolverBase {
     int run() override {
         const auto started = std::chrono::steady_clock::now();
         bool timed_out = false;
-        if (runs++ > 0 && !exec && p.use_halpern && capture_block() != cudaSuccess) return int(cudaErrorUnknown);
+        if (runs++ > 0 && !exec && !mega && p.use_halpern && capture_block() != cudaSuccess)
+            return int(cudaErrorUnknown);
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
         if (!mirror->terminated && vanilla_phase() && (st = run_vanilla(started, timed_out)) != cudaSuccess)
@@ -1820,12 +2070,12 @@ struct Solver final : SolverBase {
             for (int kk = 0; kk < 2; ++kk) {
                 if ((st = launch_block()) != cudaSuccess) return int(st);
                 if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
-                nlaunch += block_nodes;
+                nlaunch += block_launches();
             }
             int kk = 0;
             for (;;) {
                 if ((st = cudaEventSynchronize(done[kk])) != cudaSuccess) return int(st);
-                if (mirror->terminated) break;
+                if (mirror->status || mirror->terminated) break;
                 if (p.verbose)
                     fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  omega %.3e\n",
                             mirror->iteration, mirror->upper, mirror->lower, mirror->gap, mirror->omega);
@@ -1835,7 +2085,7 @@ struct Solver final : SolverBase {
                 }
                 if ((st = launch_block()) != cudaSuccess) return int(st);
                 if ((st = cudaEventRecord(done[kk], stream)) != cudaSuccess) return int(st);
-                nlaunch += block_nodes;
+                nlaunch += block_launches();
                 kk ^= 1;
             }
         }
@@ -1845,6 +2095,7 @@ struct Solver final : SolverBase {
         if ((st = cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
             (st = cudaStreamSynchronize(stream)) != cudaSuccess)
             return int(st);
+        if (mirror->status) return kMegaWaitError;
         return timed_out && !mirror->terminated ? kStatusTimeLimit : 0;
     }
 
@@ -1867,7 +2118,11 @@ struct Solver final : SolverBase {
                 profiling = false;
                 return int(st);
             }
-            nlaunch += block_nodes;
+            nlaunch += block_launches();
+            if (mirror->status) {
+                profiling = false;
+                return kMegaWaitError;
+            }
             for (auto& mk : marks) {
                 float tm = 0.f;
                 if ((st = cudaEventElapsedTime(&tm, evpool[mk.second], evpool[mk.second + 1])) != cudaSuccess) {

@@ -155,10 +155,15 @@ int reform_pria_result(reform_pria_solver* solver, double* x, double* y, double*
 
 int reform_pria_run_profiled(reform_pria_solver* solver, double* ms, int64_t* count) {
     if (!solver || !solver->impl || !ms || !count) return int(cudaErrorInvalidValue);
-    long long c[8];
+    long long c[9];
     const int st = solver->impl->run_profiled(ms, c);
-    for (int q = 0; q < 8; ++q) count[q] = c[q];
+    for (int q = 0; q < 9; ++q) count[q] = c[q];
     return st;
+}
+
+int reform_pria_set_megakernel(reform_pria_solver* solver, int mode, int* active) {
+    if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
+    return solver->impl->set_megakernel(mode, active);
 }
 
 int64_t reform_pria_launches(const reform_pria_solver* solver) {

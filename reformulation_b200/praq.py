@@ -149,7 +149,17 @@ class DeviceSolver:
 
     #: kernel kinds of `run_profiled`, in the order the C ABI reports them
     KINDS = ("node", "edge", "node_check", "edge_check", "lower", "check",
-             "restart_node", "restart_edge", "restart_check")
+             "restart_node", "restart_edge", "restart_check", "mega_block")
+
+    def set_megakernel(self, mode: int = -1) -> bool:
+        """-1: automatic (small instances), 0: the per-kernel graph, 1: the
+        persistent kernel wherever the instance allows it.  Returns whether
+        later runs take the persistent kernel."""
+        active = ctypes.c_int(0)
+        st = self._lib.reform_praq_set_megakernel(self._h, int(mode), ctypes.byref(active))
+        if st != 0:
+            raise RuntimeError(f"reform_praq_set_megakernel failed with status {st}")
+        return bool(active.value)
 
     def run_profiled(self) -> tuple[int, dict]:
         """A solve with an event pair around every kernel launch; returns the

@@ -100,7 +100,7 @@ class Library:
 class DeviceSolver:
     """A JRP instance laid out on the device once and solved repeatedly."""
 
-    KINDS = ("x", "yz", "x_check", "yz_check", "upper", "lower", "check", "restart")
+    KINDS = ("x", "yz", "x_check", "yz_check", "upper", "lower", "check", "restart", "mega_block")
 
     def __init__(self, instance, parameters=None, precision: str = "fp64", stream: int | None = None):
         self._lib = _native.lib()
@@ -122,6 +122,16 @@ class DeviceSolver:
         st = self._lib.reform_pria_set_time_limit(self._h, float(seconds))
         if st != 0:
             raise RuntimeError(f"reform_pria_set_time_limit failed with status {st}")
+
+    def set_megakernel(self, mode: int = -1) -> bool:
+        """-1: automatic (small instances), 0: the per-kernel graph, 1: the
+        persistent kernel wherever the instance allows it.  Returns whether
+        later runs take the persistent kernel."""
+        active = ctypes.c_int(0)
+        st = self._lib.reform_pria_set_megakernel(self._h, int(mode), ctypes.byref(active))
+        if st != 0:
+            raise RuntimeError(f"reform_pria_set_megakernel failed with status {st}")
+        return bool(active.value)
 
     def set_warm(self, x, y, z) -> None:
         self._warm = [np.ascontiguousarray(a, np.float64) for a in (x, y, z)]

@@ -26,6 +26,12 @@ def mix():
 
 
 def solo(qs, js, precision, tol):
+    """Each instance alone.  A small JRP alone may run in the persistent
+    kernel, whose FP32 z sums are taken over 256-thread CTAs (the batched
+    engine's over 512, as the per-kernel graph's): FP32 solos take the graph,
+    as the reference compares its batch with PRIA_MEGA=0 solos
+    (jrp/pria-cuda/src/solver.cuh:635-641); FP64 solos keep the automatic
+    choice, whose results are the graph's bit for bit."""
     from reformulation_b200 import praq, pria
     ql, jl = praq.Library(), pria.Library()
     out_q, out_j = [], []
@@ -36,6 +42,8 @@ def solo(qs, js, precision, tol):
             out_q.append(d.result())
     for j in js:
         with pria.DeviceSolver(j, jl.parameters(20000, tol), precision) as d:
+            if precision == "mixed":
+                d.set_megakernel(0)
             assert d.run() == 0
             out_j.append(d.result(want_solution=True))
     return out_q, out_j

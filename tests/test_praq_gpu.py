@@ -370,3 +370,110 @@ def test_beyond_two_to_the_26_nodes(native, oracle_lib):
     assert s.lower <= opt + 1e-9 * abs(opt) and s.upper >= opt - 1e-9 * abs(opt)
     assert rel(s.upper, opt) <= 1e-6
     assert np.all((s.x >= 0) & (s.x <= 1))
+
+
+# ---- the persistent kernel for small instances ---------------------------------
+# One cooperative launch per check block, the graph's tile functions in the
+# graph's order with the graph's CTA shape: results equal the graph's bit for
+# bit, and two runs equal each other (a grid-barrier race would break that),
+# as the reference checks its PRIA megakernel (jrp/pria-cuda/tests/
+# test_solver.cu:234-278).
+
+def _praq_runs(inst, p, mode, runs=1, warm=None):
+    from reformulation_b200.praq import DeviceSolver
+    out = []
+    with DeviceSolver(inst, p) as dev:
+        active = dev.set_megakernel(mode)
+        for _ in range(runs):
+            assert dev.run() == 0
+            out.append(dev.result(want_x=True, want_dual=True))
+        if warm is not None:
+            dev.set_warm(*warm)
+            assert dev.run() == 0
+            out.append(dev.result(want_x=True, want_dual=True))
+        launches = dev.launches()
+    return active, out, launches
+
+
+@pytest.mark.parametrize("use_float32", [0, 1])
+@pytest.mark.parametrize("shape", ["n200", "n700", "n3000", "n12000"])
+def test_persistent_kernel_equals_graph(native, use_float32, shape):
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import Library
+    inst = {"n200": lambda: qubo_sparse_bernoulli(0, 200, 0.05),
+            "n700": lambda: qubo_uniform_edges(3, 700, 2000),
+            "n3000": lambda: qubo_uniform_edges(2, 3000, 24000),
+            "n12000": lambda: qubo_uniform_edges(4, 12000, 150000)}[shape]()
+    p = Library().parameters(tolerance=1e-4 if use_float32 else 1e-7, use_float32=use_float32,
+                             max_iter=100_000)
+    rng = np.random.default_rng(1)
+    warm = (rng.uniform(0, 1, inst.n), rng.normal(0, 5, (inst.edges, 2)))
+    on, mega, ml = _praq_runs(inst, p, 1, runs=2, warm=warm)
+    off, graph, gl = _praq_runs(inst, p, 0, runs=1, warm=warm)
+    assert on and not off
+    for (a, ya), (b, yb) in ((mega[0], mega[1]), (mega[0], graph[0]), (mega[2], graph[1])):
+        assert (a.iterations, a.lower, a.upper) == (b.iterations, b.lower, b.upper)
+        assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
+    assert ml < gl
+
+
+def test_persistent_kernel_choice_and_edgeless(native):
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import DeviceSolver, Library
+    p = Library().parameters(tolerance=1e-6)
+    with DeviceSolver(qubo_sparse_bernoulli(0, 200, 0.05), p) as dev:
+        assert dev.set_megakernel(-1)                  # a few KB: automatic
+    with DeviceSolver(qubo_uniform_edges(1, 100_000, 1_000_000), p) as dev:
+        assert not dev.set_megakernel(-1)              # tens of MB: the graph
+    inst = QuboInstance("e", "e", 5, np.array([-2.0, 1.0, 3.0, -1.0, 0.0]), np.zeros(0, np.int64),
+                        np.zeros(0, np.int64), np.zeros(0))
+    with DeviceSolver(inst, Library().parameters(tolerance=1e-9, max_iter=10_000)) as dev:
+        assert dev.set_megakernel(1)
+        for _ in range(2):
+            assert dev.run() == 0
+            assert abs(dev.result().upper - (-3.0)) <= 1e-8
+
+
+def test_persistent_kernel_time_limit(native):
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = qubo_uniform_edges(5, 3000, 24000)
+    with DeviceSolver(inst, Library().parameters(tolerance=1e-14, max_iter=-1)) as dev:
+        assert dev.set_megakernel(1)
+        dev.set_time_limit(0.0)
+        assert dev.run() == 2                          # PRAQ_STATUS_TIME_LIMIT
+        r = dev.result()
+        assert r.lower <= r.upper
+
+
+def test_persistent_kernel_barrier_wait_runs_out(native):
+    """Every barrier of the persistent kernel also waits for one CTA that is
+    never launched (REFORM_PRAQ_MEGA_PHANTOM=1, a 50 ms wait limit): the first
+    wait runs out, the kernel ends, the run returns PRAQ_ERROR_CUDA, and the
+    same process then solves on the graph with the result of a clean
+    process."""
+    import os
+    import subprocess
+    import sys
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import Library
+    code = (
+        "from reformulation_b200.praq import DeviceSolver, Library\n"
+        "from reformulation_b200.instances import qubo_uniform_edges\n"
+        "inst = qubo_uniform_edges(2, 3000, 24000)\n"
+        "p = Library().parameters(tolerance=1e-6)\n"
+        "with DeviceSolver(inst, p) as dev:\n"
+        "    assert dev.set_megakernel(1)\n"
+        "    st = dev.run()\n"
+        "    assert st == -3, st\n"
+        "    assert not dev.set_megakernel(0)\n"
+        "    assert dev.run() == 0\n"
+        "    a = dev.result()\n"
+        "print(a.iterations, repr(a.upper), repr(a.lower))\n")
+    env = dict(os.environ, REFORM_PRAQ_MEGA_PHANTOM="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    it, up, lo = out.stdout.split()[-3:]
+    lib = Library()
+    ref = lib.solve(qubo_uniform_edges(2, 3000, 24000), lib.parameters(tolerance=1e-6))
+    assert int(it) == ref.iterations and float(up) == ref.upper and float(lo) == ref.lower

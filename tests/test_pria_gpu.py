@@ -266,6 +266,7 @@ def test_z_block_pairs_equal_single_blocks(native, monkeypatch, precision, shape
     for pair in ("0", "1"):
         monkeypatch.setenv("REFORM_PRIA_ZPAIR", pair)
         with pria.DeviceSolver(inst, p, precision) as dev:
+            dev.set_megakernel(0)      # the graph's z kernel in both forms
             assert dev.run() == 0
             out[pair] = dev.result(want_solution=True)
     a, b = out["0"], out["1"]
@@ -337,3 +338,144 @@ def test_time_limit_stops_with_a_valid_bracket(native, oracle_lib):
     assert res.iterations > 0
     ok = pria.solve(jrp_demand(3, 8, 30), tolerances=Tolerances(optimality=1e-6), time_limit=60.0)
     assert ok.status == "optimal"
+
+
+# ---- the persistent kernel for small instances ---------------------------------
+# The reference's checks (jrp/pria-cuda/tests/test_solver.cu:234-278): two
+# persistent-kernel runs are bitwise identical (a grid-barrier race would break
+# that) and agree with the per-kernel path.  Here the FP64 persistent kernel
+# runs the graph's tile functions in the graph's order with the same CTA
+# shapes, so the agreement is bit for bit; FP32 z sums are taken over
+# 256-thread CTAs (512 in the graph), so FP32 agrees within the objective
+# tolerance.
+
+def _mega_solve(inst, p, precision, mode, runs=1):
+    from reformulation_b200 import pria
+    out = []
+    with pria.DeviceSolver(inst, p, precision) as dev:
+        active = dev.set_megakernel(mode)
+        for _ in range(runs):
+            assert dev.run() == 0
+            out.append(dev.result(want_solution=True))
+        launches = dev.launches()
+    return active, out, launches
+
+
+def _same(a, b):
+    assert a.iterations == b.iterations
+    assert a.primal_objective == b.primal_objective and a.dual_objective == b.dual_objective
+    for k in ("x", "y", "z"):
+        assert np.array_equal(getattr(a, k), getattr(b, k))
+
+
+@pytest.mark.parametrize("shape", [(10, 25), (30, 75), (4, 12), (7, 9)])
+def test_persistent_kernel_equals_graph_fp64(native, shape):
+    from reformulation_b200 import pria
+    inst = jrp_demand(40 + shape[0], *shape)
+    p = pria.Library().parameters(-1, 1e-7)
+    on, (m1, m2), mega_launches = _mega_solve(inst, p, "fp64", 1, runs=2)
+    off, (g,), graph_launches = _mega_solve(inst, p, "fp64", 0)
+    assert on and not off
+    _same(m1, m2)                      # deterministic
+    _same(m1, g)                       # the graph's result, bit for bit
+    assert mega_launches < graph_launches
+    assert m1.relative_gap <= 1e-7
+
+
+@pytest.mark.parametrize("shape", [(10, 25), (30, 75)])
+def test_persistent_kernel_fp32(native, shape):
+    from reformulation_b200 import pria
+    inst = jrp_demand(50 + shape[0], *shape)
+    p = pria.Library().parameters(-1, 1e-4)
+    on, (m1, m2), _ = _mega_solve(inst, p, "mixed", 1, runs=2)
+    assert on
+    _same(m1, m2)
+    _, (g,), _ = _mega_solve(inst, p, "mixed", 0)
+    _, (f,), _ = _mega_solve(inst, p, "fp64", 0)
+    assert abs(m1.iterations - g.iterations) <= 2 * p.op_steps
+    assert rel(m1.primal_objective, f.primal_objective) <= 1e-6
+    assert rel(m1.primal_objective, g.primal_objective) <= 1e-6
+    feasible(inst, m1, tol=1e-6)
+
+
+@pytest.mark.parametrize("mode", PLAIN_MODES, ids=["vanilla-cap", "vanilla-tol", "warm3", "warm-past-cap"])
+def test_persistent_kernel_vanilla_and_warm_phase(native, mode):
+    """The vanilla blocks (plain PDHG, the warm phase) in the persistent kernel
+    equal the graph's, FP64, bit for bit."""
+    from reformulation_b200 import pria
+    inst = jrp_demand(60, 5, 12)
+    p = pria.Library().parameters(mode.get("max_iter", -1), mode["tolerance"],
+                                  **{k: v for k, v in mode.items() if k not in ("max_iter", "tolerance")})
+    on, (m,), _ = _mega_solve(inst, p, "fp64", 1)
+    _, (g,), _ = _mega_solve(inst, p, "fp64", 0)
+    assert on
+    _same(m, g)
+
+
+def test_persistent_kernel_choice(native):
+    """Automatic: on for at most 16,384 packed entries, off above; forced on
+    wherever one CTA holds every z period block, with the graph's result;
+    never where it does not."""
+    from reformulation_b200 import pria
+    p = pria.Library().parameters(64, 1e-12)
+    with pria.DeviceSolver(jrp_demand(70, 10, 25), p, "fp64") as dev:
+        assert dev.set_megakernel(-1)
+    big = jrp_demand(71, 60, 200)           # nd = 1.2M, one z block = 96,000 bytes in FP64
+    with pria.DeviceSolver(big, p, "fp64") as dev:
+        assert not dev.set_megakernel(-1)
+    on, (m,), _ = _mega_solve(big, p, "fp64", 1)
+    _, (g,), _ = _mega_solve(big, p, "fp64", 0)
+    assert on and m.iterations == 64
+    _same(m, g)
+    with pria.DeviceSolver(jrp_demand(72, 300, 60), p, "fp64") as dev:   # z block 0: 144,000 bytes
+        assert not dev.set_megakernel(1)
+
+
+def test_persistent_kernel_time_limit_and_cap(native):
+    from reformulation_b200 import pria
+    inst = jrp_demand(73, 30, 75)
+    _, (s,), _ = _mega_solve(inst, pria.Library().parameters(64, 1e-12), "fp64", 1)
+    assert s.iterations == 64
+    with pria.DeviceSolver(inst, pria.Library().parameters(-1, 1e-14), "fp64") as dev:
+        assert dev.set_megakernel(1)
+        dev.set_time_limit(0.0)
+        assert dev.run() == pria.TIME_LIMIT
+        r = dev.result()
+        assert r.dual_objective <= r.primal_objective
+
+
+def test_persistent_kernel_barrier_wait_runs_out(native):
+    """Fault injection on the host side of the barrier: every barrier of the
+    persistent kernel also waits for one CTA that is never launched
+    (REFORM_PRIA_MEGA_PHANTOM=1, a 50 ms wait limit), so the first wait runs
+    out; the kernel ends, the run returns cudaErrorLaunchTimeout (702), and
+    the same process then solves on the graph and, with the injection off,
+    with a new solver in the persistent kernel, with the results of a clean
+    process."""
+    import os
+    import subprocess
+    import sys
+    from reformulation_b200 import pria
+    code = (
+        "from reformulation_b200 import pria\n"
+        "from reformulation_b200.instances import jrp_demand\n"
+        "inst = jrp_demand(74, 10, 25)\n"
+        "p = pria.Library().parameters(-1, 1e-6)\n"
+        "with pria.DeviceSolver(inst, p, 'fp64') as dev:\n"
+        "    assert dev.set_megakernel(1)\n"
+        "    st = dev.run()\n"
+        "    assert st == 702, st\n"
+        "    assert not dev.set_megakernel(0)\n"
+        "    assert dev.run() == 0\n"
+        "    a = dev.result()\n"
+        "import os\n"
+        "os.environ['REFORM_PRIA_MEGA_PHANTOM'] = '0'\n"
+        "s = pria.Library().solve(inst, p)\n"
+        "print(a.iterations, repr(a.primal_objective), s.iterations, repr(s.primal_objective))\n")
+    env = dict(os.environ, REFORM_PRIA_MEGA_PHANTOM="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    it_a, obj_a, it_s, obj_s = out.stdout.split()[-4:]
+    ref = pria.Library().solve(jrp_demand(74, 10, 25), pria.Library().parameters(-1, 1e-6))
+    assert int(it_a) == int(it_s) == ref.iterations
+    assert float(obj_a) == float(obj_s) == ref.primal_objective
