@@ -132,19 +132,25 @@ REFORM_API int reform_praq_set_time_limit(reform_praq_solver* solver, double sec
  * Returns the status like reform_praq_run. */
 REFORM_API int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* count);
 
-/* Small instances: a check block runs as ONE cooperative launch whose phases
- * (node step; edge step; lower bound; check; restart step) are separated by
- * grid barriers -- a grid of one CTA for a few hundred nodes -- in place of
- * the captured graph of one kernel per phase.  No counterpart in the
- * reference's praq-cuda; its pria-cuda has one (PRIA_MEGA).  `mode` -1:
- * automatic (the default; on when a step's arrays take at most 2 MB), 0: off,
- * 1: on whenever the instance allows it (the slot-1 push layout, i.e. edge
- * arrays within twice the L2 size).  REFORM_PRAQ_MEGA=0|1 in the environment
- * sets the mode at creation.  *active (may be NULL) receives 1 when later runs
- * take the persistent kernel.  Results equal the graph's bit for bit (the same
- * tile functions, CTA shape and sums).  Every barrier wait is bounded (1 s of
- * device time): one that runs out ends the launch and the run returns
- * PRAQ_ERROR_CUDA with the context still usable. */
+/* Small instances: the persistent kernel, in place of the captured graph of
+ * one kernel per phase, in two forms.  The single-CTA form copies the whole
+ * instance into one CTA's shared memory (up to about 3,000 edges in FP64,
+ * 5,000 in FP32) and runs the start step and up to 128 check blocks per
+ * launch there, with block barriers between phases.  The grid form runs one
+ * check block per cooperative launch with its phases (node step; edge step;
+ * lower bound; check; restart step) separated by grid barriers.  No
+ * counterpart in the reference's praq-cuda; its pria-cuda has a megakernel
+ * (PRIA_MEGA).  `mode` -1: automatic (the default: the single-CTA form for
+ * at most 2,048 edges, where it measured 1.5-2x faster per solve than the
+ * graph, else the graph), 0: the graph, 1: the single-CTA form
+ * when the instance fits, else the grid form, 2: the grid form.  Both forms
+ * need the slot-1 push layout (edge arrays within twice the L2 size).
+ * REFORM_PRAQ_MEGA=0|1 in the environment sets the mode at creation.
+ * *active (may be NULL) receives the form later runs take: 0 the graph, 1 the
+ * grid form, 2 the single-CTA form.  Results equal the graph's bit for bit
+ * (the same tile functions, tile shapes and sums).  Every grid-barrier wait is
+ * bounded (1 s of device time): one that runs out ends the launch and the run
+ * returns PRAQ_ERROR_CUDA with the context still usable. */
 REFORM_API int reform_praq_set_megakernel(reform_praq_solver* solver, int mode, int* active);
 
 /* Kernel launches the last run issued (graph kernel nodes included). */

@@ -193,6 +193,16 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, unsigned expect, unsigned 
     return ok != 0;
 }
 
+// Arithmetic with its rounding fixed.  The compiler may fuse a multiply and an
+// add of a plain expression differently in different kernels (which of two
+// products to fuse, a select of products, a product by two turned into an
+// add); rmul never fuses and rfma always does, so a step written with them
+// gives the same bits in every kernel that runs it.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) {
     return v < lo ? lo : (v > hi ? hi : v);

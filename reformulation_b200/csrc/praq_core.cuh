@@ -358,15 +358,15 @@ __device__ __forceinline__ void node_kernel_tile(const Dev<Real>& d, int tile, c
         if (Reflect) {
             const double k = double(c->restart_iter + step + 1);
             const Real lw = Real(k / (k + 1.0)), rw = Real(1.0 / (k + 1.0));
-            x1v = lw * (Real(2) * x2o - x1o) + rw * x0o;
+            x1v = rfma(lw, rfma(Real(2), x2o, -x1o), rmul(rw, x0o));
         } else {
             x1v = x2o;
         }
         const Real ps = Real(kEta / c->omega);
-        const Real x2v = clampv(x1v - ps * ((di - s) / dg), Real(0), Real(1));
+        const Real x2v = clampv(rfma(-ps, (di - s) / dg, x1v), Real(0), Real(1));
         d.x1[i] = x1v;
         d.x2[i] = x2v;
-        d.r[i] = Real(2) * x2v - x1v;
+        d.r[i] = rfma(Real(2), x2v, -x1v);
         if (!Reflect) d.x0[i] = x1v;
         if (Check) {
             const double dx = double(x1v) - double(x2v);
@@ -435,9 +435,9 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
         if (e >= d.m) continue;
         const bool cov = sw[t] > Real(0);
         const Real w = cov ? sw[t] : -sw[t];
-        const Real u2 = cov ? clampv(u1[t] + hs * ((Real(1) - ri[t]) - rj[t]), -w, Real(0))
-                            : clampv(u1[t] + hs * (rj[t] - ri[t]), Real(0), w);
-        const Real nx = lwn * (Real(2) * u2 - u1[t]) + rwn * u0[t];
+        const Real u2 = cov ? clampv(rfma(hs, (Real(1) - ri[t]) - rj[t], u1[t]), -w, Real(0))
+                            : clampv(rfma(hs, rj[t] - ri[t], u1[t]), Real(0), w);
+        const Real nx = rfma(lwn, rfma(Real(2), u2, -u1[t]), rmul(rwn, u0[t]));
         d.pred[e] = nx;
         d.pred1[at1[t]] = cov ? nx : w - nx;
         if (!Reflect) d.u0[e] = u1[t];
@@ -450,13 +450,13 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
             const double x1j = d.x1[ij[t].y], x2j = d.x2[ij[t].y];
             const double dy = double(u1[t]) - double(u2);
             const double dxi = x1i - x2i, dxj = x1j - x2j;
-            acc[0] += 2.0 * dy * dy;
-            acc[1] += (cov ? dxi + dxj : dxi - dxj) * dy;
+            acc[0] += rmul(rmul(2.0, dy), dy);
+            acc[1] += rmul(cov ? dxi + dxj : dxi - dxj, dy);
             const double dr = double(u1[t]) - double(u0[t]);
-            acc[2] += 2.0 * dr * dr;
+            acc[2] += rmul(rmul(2.0, dr), dr);
             const double bi = bounds_at_1 ? x1i : x2i, bj = bounds_at_1 ? x1j : x2j;
             const double wd = double(w);
-            acc[3] += cov ? wd * fmax(bi + bj - 1.0, 0.0) : -wd * fmin(bi, bj);
+            acc[3] += cov ? rmul(wd, fmax(bi + bj - 1.0, 0.0)) : -rmul(wd, fmin(bi, bj));
             acc[4] += cov ? double(bounds_at_1 ? u1[t] : u2) : 0.0;
         }
     }
@@ -613,63 +613,425 @@ struct MegaArgs {
 
 template <class Real, bool Reflect, bool Check, bool Wide>
 __device__ __forceinline__ void mega_node(const Dev<Real>& d, const MegaArgs& a, const Real* ys, const Real* yc,
-                                          int step, int gate) {
+                                          int step, int gate, int bounds_at_1 = 0) {
     for (int t = int(blockIdx.x); t < a.nb_node; t += gridDim.x) {
-        node_kernel_tile<Real, Reflect, Check, Wide, false>(d, t, ys, yc, step, 0, gate);
+        node_kernel_tile<Real, Reflect, Check, Wide, false>(d, t, ys, yc, step, bounds_at_1, gate);
         __syncthreads();   // the next tile reuses the staging buffer
     }
 }
 
 template <class Real, bool Reflect, bool Check>
 __device__ __forceinline__ void mega_edge(const Dev<Real>& d, const MegaArgs& a, const Real* ysrc, int step,
-                                          int gate) {
+                                          int gate, int bounds_at_1 = 0) {
     for (int t = int(blockIdx.x); t < a.nb_edge; t += gridDim.x) {
-        edge_kernel_tile<Real, Reflect, Check, false>(d, t, ysrc, step, 0, gate);
+        edge_kernel_tile<Real, Reflect, Check, false>(d, t, ysrc, step, bounds_at_1, gate);
         __syncthreads();
     }
+}
+
+template <class Real, bool Wide>
+__device__ __forceinline__ void mega_lower(const Dev<Real>& d, const MegaArgs& a, const Real* ys, const Real* yc) {
+    for (int t = int(blockIdx.x); t < a.nb_node; t += gridDim.x) {
+        lower_kernel_tile<Real, Wide, false>(d, t, ys, yc);
+        __syncthreads();
+    }
+}
+
+// One check block (enqueue_steps' kernels, in their order); false when a
+// barrier ran out.  `sync` is the barrier between phases.
+template <class Real, bool Wide, class Sync>
+__device__ __forceinline__ bool mega_block_body(const Dev<Real>& d, const Params& prm, const MegaArgs& a,
+                                                Sync& sync) {
+    const int op = int(prm.op_steps);
+    for (int s = 0; s < op; ++s) {
+        if (s + 1 < op)
+            mega_node<Real, true, false, Wide>(d, a, d.pred, d.pred1, s, 0);
+        else
+            mega_node<Real, true, true, Wide>(d, a, d.pred, d.pred1, s, 0);
+        if (!sync()) return false;
+        if (d.m) {
+            if (s + 1 < op)
+                mega_edge<Real, true, false>(d, a, nullptr, s, 0);
+            else
+                mega_edge<Real, true, true>(d, a, nullptr, s, 0);
+            if (!sync()) return false;
+        }
+    }
+    mega_lower<Real, Wide>(d, a, d.u2s, d.u2s1);
+    if (!sync()) return false;
+    if (blockIdx.x == 0)
+        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 1);
+    if (!sync()) return false;
+    if (!d.ctl->restart) return true;   // uniform: the check above is the last writer
+    mega_node<Real, false, true, Wide>(d, a, d.u2s, d.u2s1, 0, 1);
+    if (!sync()) return false;
+    if (d.m) {
+        mega_edge<Real, false, true>(d, a, d.u2s, 0, 1);
+        if (!sync()) return false;
+    }
+    if (blockIdx.x == 0)
+        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 2);
+    return true;
 }
 
 // The push layout only (the slot-1 pull layout is for edge arrays beyond L2).
 template <class Real, bool Wide>
 __global__ void __launch_bounds__(kBlock, 1)
 mega_block_kernel(const __grid_constant__ Dev<Real> d, const __grid_constant__ Params prm, MegaArgs a) {
-    const int op = int(prm.op_steps);
     auto sync = [&]() {
         if (grid_sync(a.bar, a.expect, a.wait_ns)) return true;
         if (threadIdx.x == 0) d.ctl->status = kMegaWaitStatus;
         return false;
     };
-    for (int s = 0; s < op; ++s) {
-        if (s + 1 < op)
-            mega_node<Real, true, false, Wide>(d, a, d.pred, d.pred1, s, 0);
-        else
-            mega_node<Real, true, true, Wide>(d, a, d.pred, d.pred1, s, 0);
-        if (!sync()) return;
-        if (d.m) {
-            if (s + 1 < op)
-                mega_edge<Real, true, false>(d, a, nullptr, s, 0);
-            else
-                mega_edge<Real, true, true>(d, a, nullptr, s, 0);
-            if (!sync()) return;
+    mega_block_body<Real, Wide>(d, prm, a, sync);
+}
+
+// ---- the whole solve in one CTA's shared memory (a few thousand edges) ----
+// For a few hundred nodes the per-kernel graph and the grid form both wait on
+// latency: the generic tiles stage every gather through L2 in 256-thread
+// CTAs.  tiny_solve_kernel copies the instance into one 1024-thread CTA's
+// shared memory and runs the start step, the check before the loop and up to
+// `max_blocks` check blocks there, with block barriers between phases, then
+// copies the iterates and the control block back.  It keeps the graph's
+// arithmetic term for term, so its results are the graph's bit for bit:
+// * a node's S^T y is its first-end run, then its second-end run, each added
+//   in order from zero (warp_runs' sums), one thread per node;
+// * edge tiles keep their shape: thread t of the block's half q works tile
+//   q (+2, +4, ...) as thread t of a 256-thread CTA would, kEdgesPerThread
+//   edges a kBlock apart, in order;
+// * per-tile check sums are block_sums over the half (butterfly in each
+//   warp, then the half's first warp adds its 8 warp totals in order), and
+//   check_body's row reductions see at most 256 rows, which 512 threads add
+//   in the order 256 threads do.
+constexpr int kTinyThreads = 512;   // 128 registers a thread (1024 threads spill)
+constexpr int kTinyParts = kTinyThreads / kBlock;
+
+struct TinyLayout {
+    size_t x1, x2, x0, r, diag, deg, row_ptr, col_ptr, ends, w, colpos, pred, pred1, u0, u2s, u2s1;
+    size_t pnode, pedge, plower, ctl, scale, total;
+};
+
+__host__ __device__ inline size_t tiny_take(size_t& at, size_t bytes) {
+    const size_t here = at;
+    at = (at + bytes + 15) & ~size_t(15);
+    return here;
+}
+
+__host__ __device__ inline TinyLayout tiny_layout(long long n, long long m, int nb_node, int nb_edge, int real) {
+    TinyLayout t{};
+    size_t at = 0;
+    t.x1 = tiny_take(at, size_t(n) * real);
+    t.x2 = tiny_take(at, size_t(n) * real);
+    t.x0 = tiny_take(at, size_t(n) * real);
+    t.r = tiny_take(at, size_t(n) * real);
+    t.diag = tiny_take(at, size_t(n) * real);
+    t.deg = tiny_take(at, size_t(n) * real);
+    t.row_ptr = tiny_take(at, size_t(n + 1) * sizeof(int));
+    t.col_ptr = tiny_take(at, size_t(n + 1) * sizeof(int));
+    t.ends = tiny_take(at, size_t(m) * sizeof(int2));
+    t.w = tiny_take(at, size_t(m) * real);
+    t.colpos = tiny_take(at, size_t(m) * sizeof(int));
+    t.pred = tiny_take(at, size_t(m) * real);
+    t.pred1 = tiny_take(at, size_t(m) * real);
+    t.u0 = tiny_take(at, size_t(m) * real);
+    t.u2s = tiny_take(at, size_t(m) * real);
+    t.u2s1 = tiny_take(at, size_t(m) * real);
+    t.pnode = tiny_take(at, size_t(nb_node) * kNodeSums * sizeof(double));
+    t.pedge = tiny_take(at, size_t(nb_edge) * kEdgeSums * sizeof(double));
+    t.plower = tiny_take(at, size_t(nb_node) * sizeof(double));
+    t.ctl = tiny_take(at, sizeof(Control));
+    t.scale = tiny_take(at, sizeof(double));
+    t.total = at;
+    return t;
+}
+
+template <class T>
+__device__ __forceinline__ void tiny_copy(T* dst, const T* src, long long count) {
+    for (long long i = threadIdx.x; i < count; i += blockDim.x) dst[i] = src[i];
+}
+
+// block_sums over this thread's 256-thread part of the block: the part's totals
+// land in out[q * K + k].  Every thread of the block calls it.
+template <int K>
+__device__ __forceinline__ void part_sums(const double (&v)[K], double* scratch, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = warp >> 3, wq = warp & 7;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double s = warp_sum(v[k]);
+        if (lane == 0) scratch[(q * K + k) * 32 + wq] = s;
+    }
+    __syncthreads();
+    if (wq == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < kBlock / 32 ? scratch[(q * K + k) * 32 + lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out[q * K + k] = s;
         }
     }
-    for (int t = int(blockIdx.x); t < a.nb_node; t += gridDim.x) {
-        lower_kernel_tile<Real, Wide, false>(d, t, d.u2s, d.u2s1);
+    __syncthreads();
+}
+
+// A run of `v` added in order from zero.
+template <class Acc, class Real>
+__device__ __forceinline__ Acc tiny_run(const int* ptr, const Real* v, int i) {
+    Acc s = Acc(0);
+    for (int k = ptr[i], e = ptr[i + 1]; k < e; ++k) s += Acc(v[k]);
+    return s;
+}
+
+// node_kernel_tile's step, term for term, one thread per node.
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void tiny_node(const Dev<Real>& d, const Real* ys, const Real* yc, int step, int bounds_at_1,
+                                          int gate, int nb_node, double* scratch, double* qout) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;
+    for (int base = 0; base < nb_node * kBlock; base += kTinyThreads) {
+        const int i = base + int(threadIdx.x);
+        double acc[kNodeSums] = {0.0, 0.0, 0.0};
+        if (i < d.n) {
+            const Real x2o = d.x2[i], di = d.diag[i], dg = d.deg[i];
+            Real x1o = Real(0), x0o = Real(0);
+            if (Reflect) {
+                x1o = d.x1[i];
+                x0o = d.x0[i];
+            }
+            const Real s0 = tiny_run<Real>(d.row_ptr, ys, i);
+            const Real s1 = tiny_run<Real>(d.col_ptr, yc, i);
+            const Real s = s0 + s1;
+            Real x1v;
+            if (Reflect) {
+                const double k = double(c->restart_iter + step + 1);
+                const Real lw = Real(k / (k + 1.0)), rw = Real(1.0 / (k + 1.0));
+                x1v = rfma(lw, rfma(Real(2), x2o, -x1o), rmul(rw, x0o));
+            } else {
+                x1v = x2o;
+            }
+            const Real ps = Real(kEta / c->omega);
+            const Real x2v = clampv(rfma(-ps, (di - s) / dg, x1v), Real(0), Real(1));
+            d.x1[i] = x1v;
+            d.x2[i] = x2v;
+            d.r[i] = rfma(Real(2), x2v, -x1v);
+            if (!Reflect) d.x0[i] = x1v;
+            if (Check) {
+                const double dx = double(x1v) - double(x2v);
+                const double dr = Reflect ? double(x1v) - double(x0o) : 0.0;
+                acc[0] = double(dg) * dx * dx;
+                acc[1] = double(dg) * dr * dr;
+                acc[2] = double(di) * double(bounds_at_1 ? x1v : x2v);
+            }
+        }
+        if (Check) {
+            part_sums<kNodeSums>(acc, scratch, qout);
+            const int tile = base / kBlock + int(threadIdx.x >> 8);
+            if ((threadIdx.x & (kBlock - 1)) == 0 && tile < nb_node)
+                for (int k = 0; k < kNodeSums; ++k) d.pnode[size_t(tile) * kNodeSums + k] = qout[(threadIdx.x >> 8) * kNodeSums + k];
+        }
+    }
+}
+
+// edge_kernel_tile's step, term for term, the tiles two at a time.
+template <class Real, bool Reflect, bool Check>
+__device__ __forceinline__ void tiny_edge(const Dev<Real>& d, const Real* ysrc, int step, int bounds_at_1, int gate,
+                                          int nb_edge, double* scratch, double* qout) {
+    const Control* c = d.ctl;
+    if (skip(c, gate)) return;
+    const Real hs = Real(0.5 * kEta * c->omega);
+    const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
+    const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
+    const int q = int(threadIdx.x >> 8), t = int(threadIdx.x & (kBlock - 1));
+    for (int tile0 = 0; tile0 < nb_edge; tile0 += kTinyParts) {
+        const int tile = tile0 + q;
+        const int base = tile * (kBlock * kEdgesPerThread) + t;
+        double acc[kEdgeSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int u = 0; u < kEdgesPerThread; ++u) {
+            const int e = base + u * kBlock;
+            if (tile >= nb_edge || e >= d.m) continue;
+            const int2 ij = d.ends[e];
+            const Real sw = d.w[e];
+            const Real u1 = Reflect ? d.pred[e] : ysrc[e];
+            const Real u0 = Reflect ? d.u0[e] : u1;
+            const int at1 = d.colpos[e];
+            const Real ri = d.r[ij.x], rj = d.r[ij.y];
+            const bool cov = sw > Real(0);
+            const Real w = cov ? sw : -sw;
+            const Real u2 = cov ? clampv(rfma(hs, (Real(1) - ri) - rj, u1), -w, Real(0))
+                                : clampv(rfma(hs, rj - ri, u1), Real(0), w);
+            const Real nx = rfma(lwn, rfma(Real(2), u2, -u1), rmul(rwn, u0));
+            d.pred[e] = nx;
+            d.pred1[at1] = cov ? nx : w - nx;
+            if (!Reflect) d.u0[e] = u1;
+            if (Check) {
+                if (Reflect) {
+                    d.u2s[e] = u2;
+                    d.u2s1[at1] = cov ? u2 : w - u2;
+                }
+                const double x1i = d.x1[ij.x], x2i = d.x2[ij.x];
+                const double x1j = d.x1[ij.y], x2j = d.x2[ij.y];
+                const double dy = double(u1) - double(u2);
+                const double dxi = x1i - x2i, dxj = x1j - x2j;
+                acc[0] += rmul(rmul(2.0, dy), dy);
+                acc[1] += rmul(cov ? dxi + dxj : dxi - dxj, dy);
+                const double dr = double(u1) - double(u0);
+                acc[2] += rmul(rmul(2.0, dr), dr);
+                const double bi = bounds_at_1 ? x1i : x2i, bj = bounds_at_1 ? x1j : x2j;
+                const double wd = double(w);
+                acc[3] += cov ? rmul(wd, fmax(bi + bj - 1.0, 0.0)) : -rmul(wd, fmin(bi, bj));
+                acc[4] += cov ? double(bounds_at_1 ? u1 : u2) : 0.0;
+            }
+        }
+        if (Check) {
+            part_sums<kEdgeSums>(acc, scratch, qout);
+            if (t == 0 && tile < nb_edge)
+                for (int k = 0; k < kEdgeSums; ++k) d.pedge[size_t(tile) * kEdgeSums + k] = qout[q * kEdgeSums + k];
+        }
+    }
+}
+
+// lower_kernel_tile's pass, term for term, one thread per node.
+template <class Real>
+__device__ __forceinline__ void tiny_lower(const Dev<Real>& d, const Real* ys, const Real* yc, int nb_node,
+                                           double* scratch, double* qout) {
+    if (d.ctl->terminated) return;
+    for (int base = 0; base < nb_node * kBlock; base += kTinyThreads) {
+        const int i = base + int(threadIdx.x);
+        double acc[1] = {0.0};
+        if (i < d.n) {
+            const double s0 = tiny_run<double>(d.row_ptr, ys, i);
+            const double s1 = tiny_run<double>(d.col_ptr, yc, i);
+            const double s = s0 + s1;
+            const double rc = double(d.diag[i]) - s;
+            acc[0] = rc < 0.0 ? rc : 0.0;
+        }
+        part_sums<1>(acc, scratch, qout);
+        const int tile = base / kBlock + int(threadIdx.x >> 8);
+        if ((threadIdx.x & (kBlock - 1)) == 0 && tile < nb_node) d.plower[tile] = qout[threadIdx.x >> 8];
+    }
+}
+
+// check_body, out of line: its row reductions hold many values at once, and
+// inlined they would hold registers through the whole step loop.
+__device__ __noinline__ void tiny_check(Control* c, const Params& prm, const double* scale, const double* pnode,
+                                        int nbn, const double* pedge, int nbe, const double* plower, int mode) {
+    check_body(c, prm, scale, pnode, nbn, pedge, nbe, plower, nbn, mode);
+}
+
+// start: run the start step and the check before the loop first (after
+// init_kernel or warm_init_kernel has set the start point in global memory).
+template <class Real>
+__global__ void __launch_bounds__(kTinyThreads, 1)
+tiny_solve_kernel(const __grid_constant__ Dev<Real> g, const __grid_constant__ Params prm, int nb_node, int nb_edge,
+                  int start, int max_blocks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Dev<Real> d;
+    __shared__ double scratch[kTinyParts * kEdgeSums * 32];
+    __shared__ double qout[kTinyParts * kEdgeSums];
+    const TinyLayout L = tiny_layout(g.n, g.m, nb_node, nb_edge, int(sizeof(Real)));
+    auto at = [&](size_t off) { return static_cast<void*>(smem_raw + off); };
+    if (threadIdx.x == 0) {
+        d = g;
+        d.x1 = static_cast<Real*>(at(L.x1));
+        d.x2 = static_cast<Real*>(at(L.x2));
+        d.x0 = static_cast<Real*>(at(L.x0));
+        d.r = static_cast<Real*>(at(L.r));
+        d.diag = static_cast<const Real*>(at(L.diag));
+        d.deg = static_cast<const Real*>(at(L.deg));
+        d.row_ptr = static_cast<const int*>(at(L.row_ptr));
+        d.col_ptr = static_cast<const int*>(at(L.col_ptr));
+        d.ends = static_cast<const int2*>(at(L.ends));
+        d.w = static_cast<const Real*>(at(L.w));
+        d.colpos = static_cast<const int*>(at(L.colpos));
+        d.pred = static_cast<Real*>(at(L.pred));
+        d.pred1 = static_cast<Real*>(at(L.pred1));
+        d.u0 = static_cast<Real*>(at(L.u0));
+        d.u2s = static_cast<Real*>(at(L.u2s));
+        d.u2s1 = static_cast<Real*>(at(L.u2s1));
+        d.pnode = static_cast<double*>(at(L.pnode));
+        d.pedge = static_cast<double*>(at(L.pedge));
+        d.plower = static_cast<double*>(at(L.plower));
+        d.ctl = static_cast<Control*>(at(L.ctl));
+        d.scale = static_cast<const double*>(at(L.scale));
+        *d.ctl = *g.ctl;
+        *static_cast<double*>(at(L.scale)) = *g.scale;
+    }
+    const long long n = g.n, m = g.m;
+    tiny_copy(static_cast<Real*>(at(L.x1)), g.x1, n);
+    tiny_copy(static_cast<Real*>(at(L.x2)), g.x2, n);
+    tiny_copy(static_cast<Real*>(at(L.x0)), g.x0, n);
+    tiny_copy(static_cast<Real*>(at(L.r)), g.r, n);
+    tiny_copy(static_cast<Real*>(at(L.diag)), g.diag, n);
+    tiny_copy(static_cast<Real*>(at(L.deg)), g.deg, n);
+    tiny_copy(static_cast<int*>(at(L.row_ptr)), g.row_ptr, n + 1);
+    tiny_copy(static_cast<int*>(at(L.col_ptr)), g.col_ptr, n + 1);
+    tiny_copy(static_cast<int2*>(at(L.ends)), g.ends, m);
+    tiny_copy(static_cast<Real*>(at(L.w)), g.w, m);
+    tiny_copy(static_cast<int*>(at(L.colpos)), g.colpos, m);
+    tiny_copy(static_cast<Real*>(at(L.pred)), g.pred, m);
+    tiny_copy(static_cast<Real*>(at(L.pred1)), g.pred1, m);
+    tiny_copy(static_cast<Real*>(at(L.u0)), g.u0, m);
+    tiny_copy(static_cast<Real*>(at(L.u2s)), g.u2s, m);
+    tiny_copy(static_cast<Real*>(at(L.u2s1)), g.u2s1, m);
+    // with no edges no edge tile writes its partial row, which the checks read
+    for (int i = threadIdx.x; i < nb_edge * kEdgeSums; i += blockDim.x)
+        static_cast<double*>(at(L.pedge))[i] = 0.0;
+    __syncthreads();
+    if (start) {
+        // x1, y1 = _raw_step(x0, y0) with the bounds at the start point
+        // (start_step's kernels), then the check before the loop
+        tiny_node<Real, false, true>(d, d.pred, d.pred1, 0, 1, 0, nb_node, scratch, qout);
+        tiny_lower<Real>(d, d.pred, d.pred1, nb_node, scratch, qout);
+        __syncthreads();
+        if (m) {
+            tiny_edge<Real, false, true>(d, d.pred, 0, 1, 0, nb_edge, scratch, qout);
+            __syncthreads();
+        }
+        tiny_check(d.ctl, prm, d.scale, d.pnode, nb_node, d.pedge, nb_edge, d.plower, 0);
         __syncthreads();
     }
-    if (!sync()) return;
-    if (blockIdx.x == 0)
-        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 1);
-    if (!sync()) return;
-    if (!d.ctl->restart) return;   // uniform: the check above is the last writer
-    mega_node<Real, false, true, Wide>(d, a, d.u2s, d.u2s1, 0, 1);
-    if (!sync()) return;
-    if (d.m) {
-        mega_edge<Real, false, true>(d, a, d.u2s, 0, 1);
-        if (!sync()) return;
+    const int op = int(prm.op_steps);
+    for (int b = 0; b < max_blocks && !d.ctl->terminated; ++b) {
+        // one check block: enqueue_steps' kernels, in their order
+        for (int s = 0; s < op; ++s) {
+            if (s + 1 < op)
+                tiny_node<Real, true, false>(d, d.pred, d.pred1, s, 0, 0, nb_node, scratch, qout);
+            else
+                tiny_node<Real, true, true>(d, d.pred, d.pred1, s, 0, 0, nb_node, scratch, qout);
+            __syncthreads();
+            if (m) {
+                if (s + 1 < op)
+                    tiny_edge<Real, true, false>(d, nullptr, s, 0, 0, nb_edge, scratch, qout);
+                else
+                    tiny_edge<Real, true, true>(d, nullptr, s, 0, 0, nb_edge, scratch, qout);
+                __syncthreads();
+            }
+        }
+        tiny_lower<Real>(d, d.u2s, d.u2s1, nb_node, scratch, qout);
+        __syncthreads();
+        tiny_check(d.ctl, prm, d.scale, d.pnode, nb_node, d.pedge, nb_edge, d.plower, 1);
+        __syncthreads();
+        if (d.ctl->restart) {
+            tiny_node<Real, false, true>(d, d.u2s, d.u2s1, 0, 0, 1, nb_node, scratch, qout);
+            __syncthreads();
+            if (m) {
+                tiny_edge<Real, false, true>(d, d.u2s, 0, 0, 1, nb_edge, scratch, qout);
+                __syncthreads();
+            }
+            tiny_check(d.ctl, prm, d.scale, d.pnode, nb_node, d.pedge, nb_edge, d.plower, 2);
+            __syncthreads();
+        }
     }
-    if (blockIdx.x == 0)
-        check_body(d.ctl, prm, d.scale, d.pnode, a.nb_node, d.pedge, a.nb_edge, d.plower, a.nb_node, 2);
+    tiny_copy(g.x1, d.x1, n);
+    tiny_copy(g.x2, d.x2, n);
+    tiny_copy(g.x0, d.x0, n);
+    tiny_copy(g.r, d.r, n);
+    tiny_copy(g.pred, d.pred, m);
+    tiny_copy(g.pred1, d.pred1, m);
+    tiny_copy(g.u0, d.u0, m);
+    tiny_copy(g.u2s, d.u2s, m);
+    tiny_copy(g.u2s1, d.u2s1, m);
+    if (threadIdx.x == 0) *g.ctl = *d.ctl;
 }
 
 // Cold start: the centroid, x = 1/2 and y_e = (-W_ij, -W_ij) / scale, which is
@@ -891,16 +1253,20 @@ struct Solver final : SolverBase {
     long long nlaunch = 0, block_nodes = 0;
     int status_override = -100;
     int runs = 0;
-    // The persistent kernel (mega_block_kernel) in place of the graph: chosen
-    // at set-up (mode -1: when a step's arrays take at most kMegaAutoBytes), or
-    // forced by set_mega; mega_grid resident CTAs.
+    // The persistent kernel in place of the graph, in its grid form
+    // (mega_block_kernel, mega_grid resident CTAs) or its single-CTA form
+    // (tiny_solve_kernel): chosen at set-up or by set_mega.
     bool mega = false;
     int mega_mode = -1;              // -1 auto, 0 off, 1 on where the instance allows it
     int mega_grid = 0;
     unsigned mega_phantom = 0;       // CTAs the barriers also wait for, never launched (fault injection)
     unsigned long long mega_wait_ns = 1000000000ull;
     PoolBuf<GridBar> bar;
-    static constexpr long long kMegaAutoBytes = 2LL << 20;
+    // The whole solve in one CTA's shared memory (tiny_solve_kernel), when the
+    // instance fits: tiny_smem bytes; up to kTinyBlocks check blocks a launch.
+    bool tiny = false, tiny_fits = false;
+    size_t tiny_smem = 0;
+    static constexpr int kTinyBlocks = 128;
 
     ~Solver() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -986,12 +1352,6 @@ struct Solver final : SolverBase {
     }
 
     // --- the persistent kernel -------------------------------------------
-    // Bytes a step streams: per edge ends, weight, colpos and four reals
-    // (w, pred, pred1, u0), per node the run pointers and seven reals.
-    long long step_bytes() const {
-        return (long long)m * (12 + 4 * (long long)sizeof(Real)) + (long long)n * (8 + 7 * (long long)sizeof(Real));
-    }
-
     cudaError_t init_mega() {
         mega_grid = 0;
         if (!allow_mega) return cudaSuccess;
@@ -1003,6 +1363,18 @@ struct Solver final : SolverBase {
             RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
             // no phase has more tiles than this: more CTAs would only wait
             mega_grid = int(std::min<long long>((long long)per_sm * sms, std::max(nb_node, m ? nb_edge : 1)));
+            // the single-CTA form: the instance in the shared memory its
+            // static arrays leave
+            auto tfn = tiny_solve_kernel<Real>;
+            cudaFuncAttributes fa{};
+            int optin = 0;
+            RB_CUDA_TRY(cudaFuncGetAttributes(&fa, tfn));
+            RB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            const size_t room = size_t(optin) > fa.sharedSizeBytes ? size_t(optin) - fa.sharedSizeBytes : 0;
+            tiny_smem = tiny_layout(n, m, nb_node, nb_edge, int(sizeof(Real))).total;
+            // check_body's row reductions keep the 256-thread order up to 256 rows
+            tiny_fits = tiny_smem <= room && nb_node <= kBlock && nb_edge <= kBlock;
+            if (tiny_fits) RB_CUDA_TRY(cudaFuncSetAttribute(tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(room)));
         }
         // REFORM_PRAQ_MEGA=0|1 sets the initial mode (tests, measurements);
         // REFORM_PRAQ_MEGA_PHANTOM=k makes every barrier wait for k CTAs that
@@ -1018,10 +1390,17 @@ struct Solver final : SolverBase {
         return set_mega(mode);
     }
 
+    // mode -1: automatic (the single-CTA form for at most kTinyAutoTiles edge
+    // tiles, else the graph: measured per solve, the single-CTA form is 2x
+    // faster than the graph at n = 200-400 and 1.5x at n = 700, m = 2,000,
+    // but 4 % slower at n = 1,500, m = 4,500; the grid form was slower than the
+    // graph from n = 400 up); 0: the graph; 1: the single-CTA form when it
+    // fits, else the grid form; 2: the grid form.
+    static constexpr int kTinyAutoTiles = 2;
     cudaError_t set_mega(int mode) {
-        mega_mode = mode < 0 ? -1 : (mode ? 1 : 0);
-        const bool want = mega_mode == 1 || (mega_mode < 0 && step_bytes() <= kMegaAutoBytes);
-        mega = want && mega_grid > 0;
+        mega_mode = mode < 0 ? -1 : (mode > 2 ? 2 : mode);
+        tiny = tiny_fits && (mega_mode == 1 || (mega_mode == -1 && nb_edge <= kTinyAutoTiles));
+        mega = !tiny && mega_mode >= 1 && mega_grid > 0;
         if (mega && !bar.ptr) {
             RB_CUDA_TRY(bar.alloc(1, stream));
             RB_CUDA_TRY(cudaMemsetAsync(bar.ptr, 0, sizeof(GridBar), stream));
@@ -1031,8 +1410,54 @@ struct Solver final : SolverBase {
 
     int set_megakernel(int mode, int* active) override {
         const cudaError_t st = set_mega(mode);
-        if (active) *active = mega ? 1 : 0;
+        if (active) *active = tiny ? 2 : (mega ? 1 : 0);
         return st == cudaSuccess ? 0 : PRAQ_ERROR_CUDA;
+    }
+
+    cudaError_t launch_tiny(int start) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(1);
+        cfg.blockDim = dim3(unsigned(kTinyThreads));
+        cfg.dynamicSmemBytes = tiny_smem;
+        cfg.stream = stream;
+        return cudaLaunchKernelEx(&cfg, tiny_solve_kernel<Real>, d, prm, nb_node, nb_edge, start, kTinyBlocks);
+    }
+
+    // A solve in the single-CTA form: the start point set in global memory,
+    // then launches of up to kTinyBlocks check blocks (the first with the
+    // start step and its check) until the solve ends; the wall-clock budget
+    // is checked between launches.
+    int run_tiny(std::chrono::steady_clock::time_point started) {
+        nlaunch = 0;
+        const int count = std::max(n, m);
+        if (warm_x.ptr || warm_y.ptr)
+            warm_init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(
+                d, d.ctl, p.omega, p.theta_initial, warm_x.ptr, warm_y.ptr, perm.ptr);
+        else
+            init_kernel<Real><<<ceil_div(count, kBlock), kBlock, 0, stream>>>(d, d.ctl, p.omega, p.theta_initial);
+        nlaunch += 1;
+        bool timed_out = false;
+        for (int first = 1;; first = 0) {
+            if (mark_begin(9) != cudaSuccess || launch_tiny(first) != cudaSuccess || mark_end() != cudaSuccess)
+                return PRAQ_ERROR_CUDA;
+            nlaunch += 1;
+            if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+                cudaStreamSynchronize(stream) != cudaSuccess)
+                return PRAQ_ERROR_CUDA;
+            if (mirror->terminated) break;
+            if (time_limit >= 0.0 &&
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() > time_limit) {
+                timed_out = true;
+                break;
+            }
+        }
+        if (timed_out) {
+            mirror->result_slot = 2;
+            status_override = PRAQ_STATUS_TIME_LIMIT;
+            return PRAQ_STATUS_TIME_LIMIT;
+        }
+        status_override = -100;
+        return mirror->gap <= p.tolerance ? 0 : 1;
     }
 
     cudaError_t launch_mega() {
@@ -1268,6 +1693,7 @@ struct Solver final : SolverBase {
 
     int run() override {
         const auto started = std::chrono::steady_clock::now();
+        if (tiny) return run_tiny(started);
         bool timed_out = false;
         // the first run launches directly; repeated runs replay a captured block
         if (runs++ > 0 && !exec && !mega && capture_block() != cudaSuccess) return PRAQ_ERROR_CUDA;
@@ -1318,6 +1744,24 @@ struct Solver final : SolverBase {
     // block.
     int run_profiled(double* ms, long long* count) override {
         for (int k = 0; k < kKinds; ++k) { ms[k] = 0.0; count[k] = 0; }
+        if (tiny) {   // each launch of the single-CTA form as one mark of kind 9
+            marks.clear();
+            profiling = true;
+            const double budget = time_limit;
+            time_limit = -1.0;
+            const int st = run_tiny(std::chrono::steady_clock::now());
+            time_limit = budget;
+            profiling = false;
+            if (st < 0) return st;
+            for (auto& mk : marks) {
+                float t = 0.f;
+                if (cudaEventElapsedTime(&t, evpool[mk.second], evpool[mk.second + 1]) != cudaSuccess)
+                    return PRAQ_ERROR_CUDA;
+                ms[mk.first] += t;
+                count[mk.first] += 1;
+            }
+            return st;
+        }
         int st = start_solve();
         if (st) return st;
         profiling = true;

@@ -151,15 +151,16 @@ class DeviceSolver:
     KINDS = ("node", "edge", "node_check", "edge_check", "lower", "check",
              "restart_node", "restart_edge", "restart_check", "mega_block")
 
-    def set_megakernel(self, mode: int = -1) -> bool:
-        """-1: automatic (small instances), 0: the per-kernel graph, 1: the
-        persistent kernel wherever the instance allows it.  Returns whether
-        later runs take the persistent kernel."""
+    def set_megakernel(self, mode: int = -1) -> int:
+        """-1: automatic, 0: the per-kernel graph, 1: the persistent kernel's
+        single-CTA form where the instance fits, else its grid form, 2: the
+        grid form.  Returns the form later runs take: 0 the graph, 1 the grid
+        form, 2 the single-CTA form."""
         active = ctypes.c_int(0)
         st = self._lib.reform_praq_set_megakernel(self._h, int(mode), ctypes.byref(active))
         if st != 0:
             raise RuntimeError(f"reform_praq_set_megakernel failed with status {st}")
-        return bool(active.value)
+        return int(active.value)
 
     def run_profiled(self) -> tuple[int, dict]:
         """A solve with an event pair around every kernel launch; returns the

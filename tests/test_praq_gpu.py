@@ -395,9 +395,10 @@ def _praq_runs(inst, p, mode, runs=1, warm=None):
     return active, out, launches
 
 
+@pytest.mark.parametrize("form", [1, 2], ids=["single-cta-or-grid", "grid"])
 @pytest.mark.parametrize("use_float32", [0, 1])
 @pytest.mark.parametrize("shape", ["n200", "n700", "n3000", "n12000"])
-def test_persistent_kernel_equals_graph(native, use_float32, shape):
+def test_persistent_kernel_equals_graph(native, use_float32, shape, form):
     from reformulation_b200.instances import qubo_uniform_edges
     from reformulation_b200.praq import Library
     inst = {"n200": lambda: qubo_sparse_bernoulli(0, 200, 0.05),
@@ -408,9 +409,10 @@ def test_persistent_kernel_equals_graph(native, use_float32, shape):
                              max_iter=100_000)
     rng = np.random.default_rng(1)
     warm = (rng.uniform(0, 1, inst.n), rng.normal(0, 5, (inst.edges, 2)))
-    on, mega, ml = _praq_runs(inst, p, 1, runs=2, warm=warm)
+    on, mega, ml = _praq_runs(inst, p, form, runs=2, warm=warm)
     off, graph, gl = _praq_runs(inst, p, 0, runs=1, warm=warm)
-    assert on and not off
+    assert off == 0
+    assert on == (2 if form == 1 and shape in ("n200", "n700") else 1)
     for (a, ya), (b, yb) in ((mega[0], mega[1]), (mega[0], graph[0]), (mega[2], graph[1])):
         assert (a.iterations, a.lower, a.upper) == (b.iterations, b.lower, b.upper)
         assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
@@ -422,28 +424,31 @@ def test_persistent_kernel_choice_and_edgeless(native):
     from reformulation_b200.praq import DeviceSolver, Library
     p = Library().parameters(tolerance=1e-6)
     with DeviceSolver(qubo_sparse_bernoulli(0, 200, 0.05), p) as dev:
-        assert dev.set_megakernel(-1)                  # a few KB: automatic
-    with DeviceSolver(qubo_uniform_edges(1, 100_000, 1_000_000), p) as dev:
-        assert not dev.set_megakernel(-1)              # tens of MB: the graph
+        assert dev.set_megakernel(-1) == 2             # fits one CTA: the single-CTA form
+    with DeviceSolver(qubo_uniform_edges(2, 3000, 24000), p) as dev:
+        assert dev.set_megakernel(-1) == 0             # does not fit: the graph
+        assert dev.set_megakernel(1) == 1              # forced: the grid form
     inst = QuboInstance("e", "e", 5, np.array([-2.0, 1.0, 3.0, -1.0, 0.0]), np.zeros(0, np.int64),
                         np.zeros(0, np.int64), np.zeros(0))
-    with DeviceSolver(inst, Library().parameters(tolerance=1e-9, max_iter=10_000)) as dev:
-        assert dev.set_megakernel(1)
-        for _ in range(2):
-            assert dev.run() == 0
-            assert abs(dev.result().upper - (-3.0)) <= 1e-8
+    for form in (1, 2):
+        with DeviceSolver(inst, Library().parameters(tolerance=1e-9, max_iter=10_000)) as dev:
+            assert dev.set_megakernel(form) == 3 - form
+            for _ in range(2):
+                assert dev.run() == 0
+                assert abs(dev.result().upper - (-3.0)) <= 1e-8
 
 
-def test_persistent_kernel_time_limit(native):
+@pytest.mark.parametrize("case", ["grid", "single-cta"])
+def test_persistent_kernel_time_limit(native, case):
     from reformulation_b200.instances import qubo_uniform_edges
     from reformulation_b200.praq import DeviceSolver, Library
-    inst = qubo_uniform_edges(5, 3000, 24000)
-    with DeviceSolver(inst, Library().parameters(tolerance=1e-14, max_iter=-1)) as dev:
-        assert dev.set_megakernel(1)
+    inst = qubo_uniform_edges(5, 3000, 24000) if case == "grid" else qubo_sparse_bernoulli(3, 300, 0.05)
+    with DeviceSolver(inst, Library().parameters(tolerance=1e-15, max_iter=-1)) as dev:
+        assert dev.set_megakernel(1) == (1 if case == "grid" else 2)
         dev.set_time_limit(0.0)
         assert dev.run() == 2                          # PRAQ_STATUS_TIME_LIMIT
         r = dev.result()
-        assert r.lower <= r.upper
+        assert r.lower <= r.upper and r.iterations > 0
 
 
 def test_persistent_kernel_barrier_wait_runs_out(native):
