@@ -29,6 +29,8 @@
 
 #include <stdint.h>
 
+#include "reform_trace.h"
+
 #ifndef REFORM_API
 #define REFORM_API __attribute__((visibility("default")))
 #endif
@@ -152,6 +154,19 @@ REFORM_API int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, 
  * bounded (1 s of device time): one that runs out ends the launch and the run
  * returns PRAQ_ERROR_CUDA with the context still usable. */
 REFORM_API int reform_praq_set_megakernel(reform_praq_solver* solver, int mode, int* active);
+
+/* The convergence trace (include/reform_trace.h): later runs write one record
+ * per convergence check into a device ring of `capacity` records (0: no
+ * trace, the default), from the start of each run.  Setting it drops the
+ * solver's captured block (the next run captures a new one).  Returns 0 or
+ * PRAQ_ERROR_CUDA. */
+REFORM_API int reform_praq_set_trace(reform_praq_solver* solver, int capacity);
+
+/* The last run's trace, oldest first: the most recent min(written, ring
+ * capacity, `capacity`) records into `out`; *total (may be NULL) receives the
+ * number the run wrote (more than the ring holds when it wrapped). */
+REFORM_API int reform_praq_trace(reform_praq_solver* solver, reform_trace_record* out, int capacity,
+                                 int64_t* total);
 
 /* Kernel launches the last run issued (graph kernel nodes included). */
 REFORM_API int64_t reform_praq_launches(const reform_praq_solver* solver);

@@ -37,6 +37,8 @@
 
 #include <stdint.h>
 
+#include "reform_trace.h"
+
 #ifndef REFORM_API
 #define REFORM_API __attribute__((visibility("default")))
 #endif
@@ -154,6 +156,20 @@ REFORM_API int reform_pria_run_profiled(reform_pria_solver* solver, double* ms, 
  * of device time): one that runs out ends the launch, and the run returns
  * cudaErrorLaunchTimeout (702) with the context still usable. */
 REFORM_API int reform_pria_set_megakernel(reform_pria_solver* solver, int mode, int* active);
+
+/* The convergence trace (include/reform_trace.h): later runs write one record
+ * per convergence check -- the start check, every op_steps block, and in the
+ * vanilla phase its blocks and its end -- into a device ring of `capacity`
+ * records (0: no trace, the default), from the start of each run.  Setting it
+ * drops the solver's captured block (the next run captures a new one).
+ * Returns 0 or a CUDA error code. */
+REFORM_API int reform_pria_set_trace(reform_pria_solver* solver, int capacity);
+
+/* The last run's trace, oldest first: the most recent min(written, ring
+ * capacity, `capacity`) records into `out`; *total (may be NULL) receives the
+ * number the run wrote. */
+REFORM_API int reform_pria_trace(reform_pria_solver* solver, reform_trace_record* out, int capacity,
+                                 int64_t* total);
 
 REFORM_API int64_t reform_pria_launches(const reform_pria_solver* solver);
 

@@ -11,6 +11,8 @@ import ctypes
 from ctypes import POINTER, c_double, c_int, c_int64, c_void_p
 from pathlib import Path
 
+import numpy as np
+
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libreform_b200.so"
 
 
@@ -97,6 +99,10 @@ def _declare(lib):
         "reform_praq_set_warm": (I, [c_void_p, P(c_double), P(c_double)]),
         "reform_praq_run_profiled": (I, [c_void_p, D, P(c_int64)]),
         "reform_praq_set_megakernel": (I, [c_void_p, c_int, P(c_int)]),
+        "reform_praq_set_trace": (I, [c_void_p, c_int]),
+        "reform_praq_trace": (I, [c_void_p, c_void_p, c_int, P(c_int64)]),
+        "reform_pria_set_trace": (I, [c_void_p, c_int]),
+        "reform_pria_trace": (I, [c_void_p, c_void_p, c_int, P(c_int64)]),
         "reform_praq_launches": (c_int64, [c_void_p]),
         "reform_praq_destroy": (None, [c_void_p]),
         "reform_praq_bounds_noalloc": (I, [c_int64, c_int64, c_void_p, c_void_p, c_void_p,
@@ -166,6 +172,24 @@ def _declare(lib):
         fn.restype = res
         fn.argtypes = args
     return lib
+
+
+# reform_trace_record (include/reform_trace.h), as a NumPy record type
+TRACE_DTYPE = np.dtype([("iteration", np.int64), ("gap", np.float64), ("error", np.float64),
+                        ("omega", np.float64), ("lower", np.float64), ("upper", np.float64),
+                        ("restart", np.int32), ("terminated", np.int32)])
+
+
+def read_trace(fn, handle, ring: int, capacity: int = 1 << 16):
+    """The last run's convergence trace through `fn` (reform_praq_trace or
+    reform_pria_trace) from a ring of `ring` records, oldest first, as a
+    TRACE_DTYPE array."""
+    total = c_int64(0)
+    out = np.zeros(capacity, TRACE_DTYPE)
+    st = fn(handle, out.ctypes.data_as(c_void_p), capacity, ctypes.byref(total))
+    if st != 0:
+        raise RuntimeError(f"reading the trace failed with status {st}")
+    return out[:min(int(total.value), ring, capacity)].copy()
 
 
 def lib():

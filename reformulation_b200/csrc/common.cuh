@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/reform_trace.h"
+
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -202,6 +204,26 @@ __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// The convergence trace: a ring of `cap` records (reform_trace_record,
+// include/reform_trace.h) in device memory, `len` written so far; the next
+// goes to len % cap.  Written by the one thread that takes a check's
+// decisions, so no ordering beyond the check's own is needed.
+__device__ __forceinline__ void trace_put(reform_trace_record* ring, int cap, long long& len, long long iteration,
+                                          double gap, double error, double omega, double lower, double upper,
+                                          int restart, int terminated) {
+    if (!ring || cap <= 0) return;
+    reform_trace_record& r = ring[len % cap];
+    r.iteration = iteration;
+    r.gap = gap;
+    r.error = error;
+    r.omega = omega;
+    r.lower = lower;
+    r.upper = upper;
+    r.restart = restart;
+    r.terminated = terminated;
+    ++len;
+}
 
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) {

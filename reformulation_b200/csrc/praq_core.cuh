@@ -87,6 +87,7 @@ struct Control {
     int restart;      // the restart step of this block is pending
     int result_slot;  // 1: (x1, u0) hold the returned point, 2: (x2, u2s)
     int status;
+    long long trace_len;   // convergence-trace records written this run
 };
 static_assert(sizeof(Control) <= 256, "a pinned mirror slot holds one Control");
 
@@ -95,6 +96,8 @@ struct Params {
     long long max_iter, op_steps;
     double beta_sufficient, beta_necessary, beta_artificial;
     double theta_target, theta_decay;
+    reform_trace_record* trace;   // the convergence-trace ring (null: none)
+    int trace_cap;
 };
 
 template <class Real>
@@ -551,6 +554,8 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* s
         c->terminated = should_stop(gap, c->iteration, p) ? 1 : 0;
         c->result_slot = 1;
         c->restart = 0;
+        trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, gap, c->fp_error, c->omega, lower, upper, -1,
+                  c->terminated);
         return;
     }
     c->iteration += p.op_steps;
@@ -579,6 +584,9 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* s
     } else {
         c->check_error = new_err;
     }
+    const int kind = (terminated || !restart) ? 0 : (sufficient ? 1 : (necessary ? 2 : 3));
+    trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, gap, new_err, c->omega, lower, upper, kind,
+              terminated ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kCheckBlock)
@@ -1068,6 +1076,7 @@ __global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta)
         c->restart = 0;
         c->result_slot = 1;
         c->status = 0;
+        c->trace_len = 0;
     }
 }
 
@@ -1118,6 +1127,7 @@ __global__ void warm_init_kernel(Dev<Real> d, Control* c, double omega, double t
         c->restart = 0;
         c->result_slot = 1;
         c->status = 0;
+        c->trace_len = 0;
     }
 }
 
@@ -1224,6 +1234,8 @@ struct SolverBase {
     // -1 auto, 0 the graph, 1 the persistent kernel where the instance allows
     // it; *active: which one later runs take
     virtual int set_megakernel(int mode, int* active) = 0;
+    virtual int set_trace(int capacity) = 0;
+    virtual int get_trace(reform_trace_record* out, int capacity, int64_t* total) = 0;
     double time_limit = -1.0;   // seconds of wall clock per run; < 0: none
 };
 
@@ -1262,6 +1274,7 @@ struct Solver final : SolverBase {
     unsigned mega_phantom = 0;       // CTAs the barriers also wait for, never launched (fault injection)
     unsigned long long mega_wait_ns = 1000000000ull;
     PoolBuf<GridBar> bar;
+    PoolBuf<reform_trace_record> trace;   // the convergence-trace ring, optional
     // The whole solve in one CTA's shared memory (tiny_solve_kernel), when the
     // instance fits: tiny_smem bytes; up to kTinyBlocks check blocks a launch.
     bool tiny = false, tiny_fits = false;
@@ -1280,6 +1293,7 @@ struct Solver final : SolverBase {
         x1.release(); x2.release(); x0.release(); r.release(); pred.release(); pred1.release();
         u0.release(); u2s.release(); u2s1.release();
         pnode.release(); pedge.release(); plower.release(); scale.release(); ctl.release(); bar.release();
+        trace.release();
         warm_x.release(); warm_y.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
@@ -1832,6 +1846,41 @@ struct Solver final : SolverBase {
     }
 
     long long launches() const override { return nlaunch; }
+
+    // The trace ring lives in the check parameters, which a captured block
+    // holds by value: a new ring drops the capture, the next run makes one.
+    int set_trace(int capacity) override {
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
+        trace.release();
+        prm.trace = nullptr;
+        prm.trace_cap = 0;
+        if (capacity > 0) {
+            if (trace.alloc(size_t(capacity), stream) != cudaSuccess) return PRAQ_ERROR_CUDA;
+            prm.trace = trace.ptr;
+            prm.trace_cap = capacity;
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        return 0;
+    }
+
+    // The last run's records, oldest first: min(written, ring, capacity) of
+    // them, the most recent; *total = records written.
+    int get_trace(reform_trace_record* out, int capacity, int64_t* total) override {
+        const long long len = mirror->trace_len;
+        if (total) *total = len;
+        if (!prm.trace || !out || capacity <= 0) return 0;
+        std::vector<reform_trace_record> ring(size_t(prm.trace_cap));
+        if (cudaMemcpyAsync(ring.data(), prm.trace, sizeof(reform_trace_record) * ring.size(), cudaMemcpyDeviceToHost,
+                            stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return PRAQ_ERROR_CUDA;
+        const long long count = std::min<long long>({len, (long long)prm.trace_cap, (long long)capacity});
+        for (long long k = 0; k < count; ++k) out[k] = ring[size_t((len - count + k) % prm.trace_cap)];
+        return 0;
+    }
 
     size_t device_bytes() const {
         size_t b = 0;

@@ -98,6 +98,16 @@ int reform_praq_run_profiled(reform_praq_solver* solver, double* ms, int64_t* co
     return st;
 }
 
+int reform_praq_set_trace(reform_praq_solver* solver, int capacity) {
+    if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
+    return solver->impl->set_trace(capacity);
+}
+
+int reform_praq_trace(reform_praq_solver* solver, reform_trace_record* out, int capacity, int64_t* total) {
+    if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
+    return solver->impl->get_trace(out, capacity, total);
+}
+
 int reform_praq_set_megakernel(reform_praq_solver* solver, int mode, int* active) {
     if (!solver || !solver->impl) return PRAQ_ERROR_ARGUMENT;
     return solver->impl->set_megakernel(mode, active);

@@ -108,6 +108,7 @@ struct Control {
     long long restart_iter, iteration;
     int terminated, restart, result_slot, status;
     int phase_done;          // the vanilla phase reached its step budget
+    long long trace_len;     // convergence-trace records written this run
 };
 
 struct Params {
@@ -120,6 +121,8 @@ struct Params {
     long long vanilla_max;   // step budget of the vanilla phase (< 0: none)
     double omega0;           // the initial primal weight
     int vanilla_solve;       // plain PDHG throughout (no Halpern phase)
+    reform_trace_record* trace;   // the convergence-trace ring (null: none)
+    int trace_cap;
 };
 
 // Bits of the `gate` argument of the step kernels.
@@ -1057,6 +1060,8 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* p
         c->phase_done = 0;
         c->result_slot = 1;   // the point the gap was measured at is now the anchor
         c->terminated = should_stop(c->gap, c->iteration, p) ? 1 : 0;
+        trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, c->gap, c->fp_error, c->omega, c->lower,
+                  c->upper, 5, c->terminated);
         return;
     }
     if (mode == 3) {
@@ -1074,6 +1079,8 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* p
             if (p.vanilla_solve) c->terminated = 1;   // a vanilla solve: its iteration limit
             else c->phase_done = 1;
         }
+        trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, gap, NAN, c->omega, lower, upper, 4,
+                  c->terminated);
         return;
     }
     if (mode == 2) {
@@ -1098,6 +1105,8 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* p
         c->terminated = should_stop(gap, c->iteration, q) ? 1 : 0;
         c->result_slot = 1;
         c->restart = 0;
+        trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, gap, c->fp_error, c->omega, lower, upper, -1,
+                  c->terminated);
         return;
     }
     c->iteration += p.op_steps;
@@ -1128,6 +1137,9 @@ __device__ __forceinline__ void check_body(Control* c, Params p, const double* p
         if (restart) c->restart = 1;
         else c->check_error = new_err;
     }
+    const int kind = (terminated || !restart) ? 0 : (sufficient ? 1 : (necessary ? 2 : 3));
+    trace_put(p.trace, p.trace_cap, c->trace_len, c->iteration, gap, new_err, c->omega, lower, upper, kind,
+              terminated ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kCheckBlock)
@@ -1294,6 +1306,7 @@ __global__ void init_kernel(Dev<Real> d, Control* c, double omega, double theta)
         c->result_slot = 1;
         c->status = 0;
         c->phase_done = 0;
+        c->trace_len = 0;
     }
 }
 
@@ -1512,6 +1525,8 @@ struct SolverBase {
     // -1 auto, 0 the graph, 1 the persistent kernel where the instance allows
     // it; *active: which one later runs take
     virtual int set_megakernel(int mode, int* active) = 0;
+    virtual int set_trace(int capacity) = 0;
+    virtual int get_trace(reform_trace_record* out, int capacity, int64_t* total) = 0;
 };
 
 template <class Real>
@@ -1546,6 +1561,7 @@ struct Solver final : SolverBase {
     unsigned mega_phantom = 0;       // CTAs the barriers also wait for, never launched (fault injection)
     unsigned long long mega_wait_ns = 1000000000ull;
     PoolBuf<GridBar> bar;
+    PoolBuf<reform_trace_record> trace;   // the convergence-trace ring, optional
     static constexpr size_t kMegaSmemLimit = 96 * 1024;
     static constexpr long long kMegaAutoEntries = 16384;
     static constexpr int kZThreadsPerCta = z_threads<Real>();
@@ -1569,6 +1585,7 @@ struct Solver final : SolverBase {
         for (auto* b : {&px, &py, &pyz, &pup, &plo, &final_up, &thx, &thy, &thz}) b->release();
         for (auto& b : warm) b.release();
         bar.release();
+        trace.release();
         ctl.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
@@ -1957,6 +1974,40 @@ struct Solver final : SolverBase {
         const cudaError_t st = set_mega(mode);
         if (active) *active = mega ? 1 : 0;
         return int(st);
+    }
+
+    // The trace ring lives in the check parameters, which a captured block
+    // holds by value: a new ring drops the capture, the next run makes one.
+    int set_trace(int capacity) override {
+        RB_CUDA_TRY(cudaStreamSynchronize(stream));
+        trace.release();
+        prm.trace = nullptr;
+        prm.trace_cap = 0;
+        if (capacity > 0) {
+            RB_CUDA_TRY(trace.alloc(size_t(capacity), stream));
+            prm.trace = trace.ptr;
+            prm.trace_cap = capacity;
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        return 0;
+    }
+
+    // The last run's records, oldest first: min(written, ring, capacity) of
+    // them, the most recent; *total = records written.
+    int get_trace(reform_trace_record* out, int capacity, int64_t* total) override {
+        const long long len = mirror->trace_len;
+        if (total) *total = len;
+        if (!prm.trace || !out || capacity <= 0) return 0;
+        std::vector<reform_trace_record> ring(size_t(prm.trace_cap));
+        RB_CUDA_TRY(cudaMemcpyAsync(ring.data(), prm.trace, sizeof(reform_trace_record) * ring.size(),
+                                    cudaMemcpyDeviceToHost, stream));
+        RB_CUDA_TRY(cudaStreamSynchronize(stream));
+        const long long count = std::min<long long>({len, (long long)prm.trace_cap, (long long)capacity});
+        for (long long k = 0; k < count; ++k) out[k] = ring[size_t((len - count + k) % prm.trace_cap)];
+        return 0;
     }
 
     int set_warm(const double* wx, const double* wy, const double* wz) override {

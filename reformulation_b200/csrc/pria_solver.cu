@@ -161,6 +161,16 @@ int reform_pria_run_profiled(reform_pria_solver* solver, double* ms, int64_t* co
     return st;
 }
 
+int reform_pria_set_trace(reform_pria_solver* solver, int capacity) {
+    if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
+    return solver->impl->set_trace(capacity);
+}
+
+int reform_pria_trace(reform_pria_solver* solver, reform_trace_record* out, int capacity, int64_t* total) {
+    if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
+    return solver->impl->get_trace(out, capacity, total);
+}
+
 int reform_pria_set_megakernel(reform_pria_solver* solver, int mode, int* active) {
     if (!solver || !solver->impl) return int(cudaErrorInvalidValue);
     return solver->impl->set_megakernel(mode, active);

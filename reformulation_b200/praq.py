@@ -151,6 +151,20 @@ class DeviceSolver:
     KINDS = ("node", "edge", "node_check", "edge_check", "lower", "check",
              "restart_node", "restart_edge", "restart_check", "mega_block")
 
+    def set_trace(self, capacity: int) -> None:
+        """Later runs record every convergence check (iteration, gap, error,
+        omega, bounds, restart decision) into a device ring of `capacity`
+        records; 0 turns it off."""
+        st = self._lib.reform_praq_set_trace(self._h, int(capacity))
+        if st != 0:
+            raise RuntimeError(f"reform_praq_set_trace failed with status {st}")
+        self._trace_ring = max(int(capacity), 0)
+
+    def trace(self, capacity: int = 1 << 16):
+        """The last run's checks, oldest first (a NumPy record array with the
+        fields of reform_trace_record)."""
+        return _native.read_trace(self._lib.reform_praq_trace, self._h, getattr(self, "_trace_ring", 0), capacity)
+
     def set_megakernel(self, mode: int = -1) -> int:
         """-1: automatic, 0: the per-kernel graph, 1: the persistent kernel's
         single-CTA form where the instance fits, else its grid form, 2: the

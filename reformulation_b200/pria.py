@@ -123,6 +123,20 @@ class DeviceSolver:
         if st != 0:
             raise RuntimeError(f"reform_pria_set_time_limit failed with status {st}")
 
+    def set_trace(self, capacity: int) -> None:
+        """Later runs record every convergence check (iteration, gap, error,
+        omega, bounds, restart decision) into a device ring of `capacity`
+        records; 0 turns it off."""
+        st = self._lib.reform_pria_set_trace(self._h, int(capacity))
+        if st != 0:
+            raise RuntimeError(f"reform_pria_set_trace failed with status {st}")
+        self._trace_ring = max(int(capacity), 0)
+
+    def trace(self, capacity: int = 1 << 16):
+        """The last run's checks, oldest first (a NumPy record array with the
+        fields of reform_trace_record)."""
+        return _native.read_trace(self._lib.reform_pria_trace, self._h, getattr(self, "_trace_ring", 0), capacity)
+
     def set_megakernel(self, mode: int = -1) -> bool:
         """-1: automatic (small instances), 0: the per-kernel graph, 1: the
         persistent kernel wherever the instance allows it.  Returns whether

@@ -5,6 +5,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import pytest
+
 ROOT = Path(__file__).resolve().parent.parent
 
 
@@ -32,6 +34,32 @@ def test_struct_layouts_match_reference_sizes():
     assert ctypes.sizeof(_native.PraqResult) == 32
     assert ctypes.sizeof(_native.PriaParams) == 9 * 8 + 8 + 4 * 4
     assert ctypes.sizeof(_native.PriaResultInfo) == 32
+
+
+def test_trace_record_layout_matches_the_header(tmp_path):
+    """reform_trace_record (include/reform_trace.h) as compiled by the host C
+    compiler has the size and field offsets of the NumPy record type the
+    Python backends read the trace into."""
+    import shutil
+    import subprocess
+    import numpy as np
+    from reformulation_b200 import _native
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    root = Path(__file__).resolve().parent.parent
+    src = tmp_path / "t.c"
+    fields = _native.TRACE_DTYPE.names
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"reform_trace.h\"\n"
+                   "int main(void) { printf(\"%zu\", sizeof(reform_trace_record));"
+                   + "".join(f" printf(\" %zu\", offsetof(reform_trace_record, {f}));" for f in fields)
+                   + " return 0; }\n")
+    exe = tmp_path / "t"
+    subprocess.run([cc, f"-I{root / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == _native.TRACE_DTYPE.itemsize
+    assert got[1:] == [_native.TRACE_DTYPE.fields[f][1] for f in fields]
+    assert np.dtype(_native.TRACE_DTYPE).itemsize == 56
 
 
 def test_default_parameters_and_interval_rule(native):

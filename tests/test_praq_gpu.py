@@ -482,3 +482,54 @@ def test_persistent_kernel_barrier_wait_runs_out(native):
     lib = Library()
     ref = lib.solve(qubo_uniform_edges(2, 3000, 24000), lib.parameters(tolerance=1e-6))
     assert int(it) == ref.iterations and float(up) == ref.upper and float(lo) == ref.lower
+
+
+def test_convergence_trace(native):
+    """The convergence trace (reform_praq_set_trace): one record per check,
+    the start check first, then every op_steps block; the last record is the
+    run's final check (its gap and bounds are the result's), restarts change
+    omega only where the record says one was taken, and the records are the
+    same in every form (graph, grid form, single CTA) and on a second run."""
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import DeviceSolver, Library
+    for inst in (qubo_sparse_bernoulli(0, 200, 0.05), qubo_uniform_edges(2, 3000, 24000)):
+        p = Library().parameters(tolerance=1e-7, max_iter=100_000)
+        traces = []
+        for mode in (0, 1, 2):
+            with DeviceSolver(inst, p) as dev:
+                dev.set_megakernel(mode)
+                dev.set_trace(4096)
+                for _ in range(2):
+                    assert dev.run() == 0
+                    r = dev.result(want_x=False)
+                    tr = dev.trace()
+                    traces.append(tr)
+        tr = traces[0]
+        op = int(p.op_steps) if p.op_steps > 0 else int(tr["iteration"][1] - tr["iteration"][0])
+        assert tr["restart"][0] == -1 and tr["iteration"][0] == 0
+        assert np.all(np.diff(tr["iteration"]) == op)
+        assert tr["terminated"][-1] == 1 and not tr["terminated"][:-1].any()
+        assert tr["iteration"][-1] == r.iterations
+        assert tr["gap"][-1] <= 1e-7 and (tr["gap"][:-1] > 1e-7).all()
+        assert tr["lower"][-1] == r.lower and tr["upper"][-1] == r.upper
+        taken = tr["restart"][1:-1] > 0
+        changed = tr["omega"][1:] != tr["omega"][:-1]
+        assert not (changed[:-1] & ~taken).any()          # omega moves only on a restart
+        for other in traces[1:]:
+            assert other.tobytes() == tr.tobytes()
+
+
+def test_convergence_trace_ring_wraps(native):
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = qubo_sparse_bernoulli(0, 200, 0.05)
+    with DeviceSolver(inst, Library().parameters(tolerance=1e-7, max_iter=100_000)) as dev:
+        dev.set_trace(4096)
+        dev.run()
+        full = dev.trace()
+        dev.set_trace(3)
+        dev.run()
+        last = dev.trace()
+        dev.set_trace(0)
+        dev.run()
+        assert len(dev.trace()) == 0
+    assert len(full) > 3 and last.tobytes() == full[-3:].tobytes()

@@ -479,3 +479,33 @@ def test_persistent_kernel_barrier_wait_runs_out(native):
     ref = pria.Library().solve(jrp_demand(74, 10, 25), pria.Library().parameters(-1, 1e-6))
     assert int(it_a) == int(it_s) == ref.iterations
     assert float(obj_a) == float(obj_s) == ref.primal_objective
+
+
+@pytest.mark.parametrize("mode", [dict(), dict(warm_steps=2)], ids=["halpern", "warm-phase"])
+def test_convergence_trace(native, mode):
+    """The convergence trace (reform_pria_set_trace): the start check, the
+    vanilla blocks and the end of the vanilla phase where there is one, then
+    one record per op_steps block; the last is the final check (the result's
+    gap and bounds); the same records on the graph and in the persistent
+    kernel (FP64) and on a second run."""
+    from reformulation_b200 import pria
+    inst = jrp_demand(80, 10, 25)
+    p = pria.Library().parameters(-1, 1e-7, **mode)
+    traces = []
+    for mega in (0, 1):
+        with pria.DeviceSolver(inst, p, "fp64") as dev:
+            dev.set_megakernel(mega)
+            dev.set_trace(1024)
+            for _ in range(2):
+                assert dev.run() == 0
+                r = dev.result()
+                traces.append(dev.trace())
+    tr = traces[0]
+    assert tr["restart"][0] == -1
+    if mode:
+        assert list(tr["restart"][1:4]) == [4, 4, 5]
+    assert tr["terminated"][-1] == 1 and not tr["terminated"][:-1].any()
+    assert tr["iteration"][-1] == r.iterations and tr["gap"][-1] <= 1e-7
+    assert np.all(np.diff(tr["iteration"]) >= 0) and (tr["gap"][:-1] > 1e-7).all()
+    for other in traces[1:]:
+        assert other.tobytes() == tr.tobytes()
