@@ -123,6 +123,10 @@ REFORM_API int reform_pria_run(reform_pria_solver* solver);
  * and the bracket of the last completed check -- a valid bracket, since every
  * iterate is feasible.  A run that converges in the same block returns 0. */
 #define REFORM_PRIA_STATUS_TIME_LIMIT (-1)
+/* Only from a library built with RB200_DEBUG_BOUNDS (python -m
+ * reformulation_b200.build --debug-bounds): an index out of range was caught
+ * and its access skipped; the result is not valid. */
+#define REFORM_PRIA_STATUS_BOUNDS (-2)
 REFORM_API int reform_pria_set_time_limit(reform_pria_solver* solver, double seconds);
 
 /* Warm start for the next runs: dense [n][t][t] FP64 arrays in the output

@@ -8,12 +8,15 @@ are byte-compatible with the reference's praq.h / pria.h).
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import POINTER, c_double, c_int, c_int64, c_void_p
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libreform_b200.so"
+# REFORM_B200_LIB names another build of the library (the checked build,
+# libreform_b200_debug_bounds.so); the default is the in-tree release build.
+LIB_PATH = Path(os.environ.get("REFORM_B200_LIB") or Path(__file__).resolve().parent / "_lib" / "libreform_b200.so")
 
 
 class PraqInstance(ctypes.Structure):

@@ -57,9 +57,9 @@ def stale() -> bool:
     return any(p.stat().st_mtime > t for p in sources() + headers())
 
 
-def _compile(src: Path, verbose: bool) -> Path:
-    obj = OBJ / (src.stem + ".o")
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+def _compile(src: Path, verbose: bool, objdir: Path = OBJ, extra: tuple = ()) -> Path:
+    obj = objdir / (src.stem + ".o")
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -94,23 +94,47 @@ def build_cli(force: bool = False) -> list[Path]:
     return out
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not stale():
-        build_cli()
-        return LIB
-    OBJ.mkdir(parents=True, exist_ok=True)
+def _link(objdir: Path, lib: Path, verbose: bool, extra: tuple = ()) -> Path:
+    objdir.mkdir(parents=True, exist_ok=True)
     srcs = sources()
     with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as pool:
-        objs = list(pool.map(lambda s: _compile(s, verbose), srcs))
-    tmp = LIB.with_suffix(".so.tmp")
+        objs = list(pool.map(lambda s: _compile(s, verbose, objdir, extra), srcs))
+    tmp = lib.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stderr}")
-    tmp.replace(LIB)
+    tmp.replace(lib)
+    return lib
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not stale():
+        build_cli()
+        return LIB
+    _link(OBJ, LIB, verbose)
     build_cli(force=True)
     return LIB
 
 
+# The checked build (RB200_DEBUG_BOUNDS, csrc/common.cuh): every gather and
+# scatter index that comes from data is range-checked on the device; a bad one
+# is skipped and reported through the run's status.  A library of its own, for
+# tests and debugging; nothing loads it unless asked (REFORM_B200_LIB).
+DEBUG_LIB = OUT / "libreform_b200_debug_bounds.so"
+DEBUG_OBJ = OUT / "obj_debug_bounds"
+
+
+def build_debug_bounds(force: bool = False, verbose: bool = False) -> Path:
+    if not force and DEBUG_LIB.exists():
+        t = DEBUG_LIB.stat().st_mtime
+        if not any(p.stat().st_mtime > t for p in sources() + headers()):
+            return DEBUG_LIB
+    return _link(DEBUG_OBJ, DEBUG_LIB, verbose, ("-DRB200_DEBUG_BOUNDS",))
+
+
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    if "--debug-bounds" in sys.argv:
+        print(build_debug_bounds(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    else:
+        print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -205,6 +205,30 @@ __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// ---- the checked build ----------------------------------------------------
+// Built with RB200_DEBUG_BOUNDS (python -m reformulation_b200.build
+// --debug-bounds, a library of its own), every gather and scatter whose index
+// comes from data is checked: index_ok() returns false for an index out of
+// range, marks the solver's control block (status = kBoundsStatus; the run
+// returns an error) and the caller skips the access, so a bad index is
+// reported instead of read or written.  In the normal build index_ok() is
+// `true` and costs nothing.
+#ifdef RB200_DEBUG_BOUNDS
+constexpr bool kDebugBounds = true;
+#else
+constexpr bool kDebugBounds = false;
+#endif
+constexpr int kBoundsStatus = 2;
+
+__device__ __forceinline__ bool index_ok(bool ok, int* status) {
+    if constexpr (kDebugBounds) {
+        if (!ok) atomicExch(status, kBoundsStatus);
+        return ok;
+    } else {
+        return true;
+    }
+}
+
 // The convergence trace: a ring of `cap` records (reform_trace_record,
 // include/reform_trace.h) in device memory, `len` written so far; the next
 // goes to len % cap.  Written by the one thread that takes a check's

@@ -152,11 +152,14 @@ constexpr int stage_len() { return RB200_PRAQ_STAGE_BYTES / int(sizeof(Real)); }
 // unrolled loop; 8 were no better).
 template <class Real, class Acc, bool Indexed>
 __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real* v, const int* __restrict__ idx,
-                                         int n, long long base, int lane, Real* __restrict__ stage) {
+                                         int n, long long base, int lane, Real* __restrict__ stage, int m,
+                                         int* status) {
     if (base >= n) return Acc(0);   // uniform over the warp
     const long long i = base + lane;
     const long long last = base + 32 < n ? base + 32 : n;
     const int lo_all = ptr[base], hi_all = ptr[last];
+    // the warp's range, the same on every lane (the runs inside it follow)
+    if (!index_ok(0 <= lo_all && lo_all <= hi_all && hi_all <= m, status)) return Acc(0);
     int a = 0, b = 0;
     if (i < n) {
         a = ptr[i];
@@ -181,7 +184,7 @@ __device__ __forceinline__ Acc warp_runs(const int* __restrict__ ptr, const Real
 #pragma unroll
                 for (int u = 0; u < kSeqChunk; ++u) {
                     const int k = k0 + lane + 32 * u;
-                    if (k < c1) t[u] = v[at[u]];
+                    if (k < c1) t[u] = index_ok(unsigned(at[u]) < unsigned(m), status) ? v[at[u]] : Real(0);
                 }
             } else {
 #pragma unroll
@@ -221,13 +224,14 @@ template <class Real, class Acc, bool IndexB>
 __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Real* va, const int* __restrict__ pb,
                                            const Real* vb, const int* __restrict__ ib, int n, long long base, int lane,
                                            Real* __restrict__ sa,
-                                           Real* __restrict__ sb, Acc& ra, Acc& rb) {
+                                           Real* __restrict__ sb, Acc& ra, Acc& rb, int m, int* status) {
     ra = Acc(0);
     rb = Acc(0);
     if (base >= n) return;   // uniform over the warp
     const long long i = base + lane;
     const long long last = base + 32 < n ? base + 32 : n;
     const int alo = pa[base], ahi = pa[last], blo = pb[base], bhi = pb[last];
+    if (!index_ok(0 <= alo && alo <= ahi && ahi <= m && 0 <= blo && blo <= bhi && bhi <= m, status)) return;
     int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
     if (i < n) {
         a0 = pa[i];
@@ -265,7 +269,7 @@ __device__ __forceinline__ void warp_runs2(const int* __restrict__ pa, const Rea
 #pragma unroll
             for (int q = 0; q < kPer; ++q) {
                 if (32 * q >= wide) break;
-                if (32 * q < nb) ta[q] = vb[at[q]];
+                if (32 * q < nb) ta[q] = index_ok(unsigned(at[q]) < unsigned(m), status) ? vb[at[q]] : Real(0);
             }
 #pragma unroll
             for (int q = 0; q < kPer; ++q) {
@@ -319,11 +323,11 @@ __device__ __forceinline__ Acc scatter_at(const Dev<Real>& d, const Real* ys, co
     if constexpr (Wide) {
         Acc s0, s1;
         warp_runs2<Real, Acc, Pull>(d.row_ptr, ys, d.col_ptr, yc, d.colidx, d.n, base, lane, stage,
-                                    stage + stage_len<Real>(), s0, s1);
+                                    stage + stage_len<Real>(), s0, s1, d.m, &d.ctl->status);
         return s0 + s1;
     } else {
-        const Acc s0 = warp_runs<Real, Acc, false>(d.row_ptr, ys, nullptr, d.n, base, lane, stage);
-        const Acc s1 = warp_runs<Real, Acc, Pull>(d.col_ptr, yc, d.colidx, d.n, base, lane, stage);
+        const Acc s0 = warp_runs<Real, Acc, false>(d.row_ptr, ys, nullptr, d.n, base, lane, stage, d.m, &d.ctl->status);
+        const Acc s1 = warp_runs<Real, Acc, Pull>(d.col_ptr, yc, d.colidx, d.n, base, lane, stage, d.m, &d.ctl->status);
         return s0 + s1;
     }
 }
@@ -427,8 +431,11 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
 #pragma unroll
     for (int t = 0; t < kEdgesPerThread; ++t) {
         if (base + t * kBlock < d.m) {
-            ri[t] = d.r[ij[t].x];
-            rj[t] = d.r[ij[t].y];
+            const bool ok = index_ok(unsigned(ij[t].x) < unsigned(d.n) && unsigned(ij[t].y) < unsigned(d.n),
+                                     &d.ctl->status);
+            ri[t] = ok ? d.r[ij[t].x] : Real(0);
+            rj[t] = ok ? d.r[ij[t].y] : Real(0);
+            if (!ok) ij[t] = make_int2(0, 0);   // the check's gathers below stay in range
         }
     }
     double acc[kEdgeSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -442,12 +449,13 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
                             : clampv(rfma(hs, rj[t] - ri[t], u1[t]), Real(0), w);
         const Real nx = rfma(lwn, rfma(Real(2), u2, -u1[t]), rmul(rwn, u0[t]));
         d.pred[e] = nx;
-        d.pred1[at1[t]] = cov ? nx : w - nx;
+        const bool oka = index_ok(unsigned(at1[t]) < unsigned(d.m), &d.ctl->status);
+        if (oka) d.pred1[at1[t]] = cov ? nx : w - nx;
         if (!Reflect) d.u0[e] = u1[t];
         if (Check) {
             if (Reflect) {
                 d.u2s[e] = u2;
-                d.u2s1[at1[t]] = cov ? u2 : w - u2;
+                if (oka) d.u2s1[at1[t]] = cov ? u2 : w - u2;
             }
             const double x1i = d.x1[ij[t].x], x2i = d.x2[ij[t].x];
             const double x1j = d.x1[ij[t].y], x2j = d.x2[ij[t].y];
@@ -783,9 +791,11 @@ __device__ __forceinline__ void part_sums(const double (&v)[K], double* scratch,
 
 // A run of `v` added in order from zero.
 template <class Acc, class Real>
-__device__ __forceinline__ Acc tiny_run(const int* ptr, const Real* v, int i) {
+__device__ __forceinline__ Acc tiny_run(const int* ptr, const Real* v, int i, int m, int* status) {
     Acc s = Acc(0);
-    for (int k = ptr[i], e = ptr[i + 1]; k < e; ++k) s += Acc(v[k]);
+    const int k0 = ptr[i], e = ptr[i + 1];
+    if (!index_ok(0 <= k0 && k0 <= e && e <= m, status)) return s;
+    for (int k = k0; k < e; ++k) s += Acc(v[k]);
     return s;
 }
 
@@ -805,8 +815,8 @@ __device__ __forceinline__ void tiny_node(const Dev<Real>& d, const Real* ys, co
                 x1o = d.x1[i];
                 x0o = d.x0[i];
             }
-            const Real s0 = tiny_run<Real>(d.row_ptr, ys, i);
-            const Real s1 = tiny_run<Real>(d.col_ptr, yc, i);
+            const Real s0 = tiny_run<Real>(d.row_ptr, ys, i, d.m, &d.ctl->status);
+            const Real s1 = tiny_run<Real>(d.col_ptr, yc, i, d.m, &d.ctl->status);
             const Real s = s0 + s1;
             Real x1v;
             if (Reflect) {
@@ -862,22 +872,26 @@ __device__ __forceinline__ void tiny_edge(const Dev<Real>& d, const Real* ysrc, 
             const Real u1 = Reflect ? d.pred[e] : ysrc[e];
             const Real u0 = Reflect ? d.u0[e] : u1;
             const int at1 = d.colpos[e];
-            const Real ri = d.r[ij.x], rj = d.r[ij.y];
+            const bool ok = index_ok(unsigned(ij.x) < unsigned(d.n) && unsigned(ij.y) < unsigned(d.n),
+                                     &d.ctl->status);
+            const int2 ijs = ok ? ij : make_int2(0, 0);   // every gather below stays in range
+            const Real ri = d.r[ijs.x], rj = d.r[ijs.y];
             const bool cov = sw > Real(0);
             const Real w = cov ? sw : -sw;
             const Real u2 = cov ? clampv(rfma(hs, (Real(1) - ri) - rj, u1), -w, Real(0))
                                 : clampv(rfma(hs, rj - ri, u1), Real(0), w);
             const Real nx = rfma(lwn, rfma(Real(2), u2, -u1), rmul(rwn, u0));
             d.pred[e] = nx;
-            d.pred1[at1] = cov ? nx : w - nx;
+            const bool oka = index_ok(unsigned(at1) < unsigned(d.m), &d.ctl->status);
+            if (oka) d.pred1[at1] = cov ? nx : w - nx;
             if (!Reflect) d.u0[e] = u1;
             if (Check) {
                 if (Reflect) {
                     d.u2s[e] = u2;
-                    d.u2s1[at1] = cov ? u2 : w - u2;
+                    if (oka) d.u2s1[at1] = cov ? u2 : w - u2;
                 }
-                const double x1i = d.x1[ij.x], x2i = d.x2[ij.x];
-                const double x1j = d.x1[ij.y], x2j = d.x2[ij.y];
+                const double x1i = d.x1[ijs.x], x2i = d.x2[ijs.x];
+                const double x1j = d.x1[ijs.y], x2j = d.x2[ijs.y];
                 const double dy = double(u1) - double(u2);
                 const double dxi = x1i - x2i, dxj = x1j - x2j;
                 acc[0] += rmul(rmul(2.0, dy), dy);
@@ -907,8 +921,8 @@ __device__ __forceinline__ void tiny_lower(const Dev<Real>& d, const Real* ys, c
         const int i = base + int(threadIdx.x);
         double acc[1] = {0.0};
         if (i < d.n) {
-            const double s0 = tiny_run<double>(d.row_ptr, ys, i);
-            const double s1 = tiny_run<double>(d.col_ptr, yc, i);
+            const double s0 = tiny_run<double>(d.row_ptr, ys, i, d.m, &d.ctl->status);
+            const double s1 = tiny_run<double>(d.col_ptr, yc, i, d.m, &d.ctl->status);
             const double s = s0 + s1;
             const double rc = double(d.diag[i]) - s;
             acc[0] = rc < 0.0 ? rc : 0.0;

@@ -295,7 +295,8 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
         for (int u = 0; u < kUnroll; ++u) {
             const int s = sb + u * rstep;
             ev[u] = -1;
-            if (s < rows && col < tcols && tt >= s) {
+            if (s < rows && col < tcols && tt >= s &&
+                index_ok(blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s) < d.nd, &d.ctl->status)) {
                 ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
                 xv[u] = xsrc[ev[u]];
                 hv[u] = d.h[ev[u]];
@@ -337,7 +338,8 @@ __device__ __forceinline__ void x_kernel_tile(const Dev<Real>& d, int tile, cons
         for (int u = 0; u < kUnroll; ++u) {
             const int s = sb + u * rstep;
             ev[u] = -1;
-            if (s < rows && col < tcols && tt >= s) {
+            if (s < rows && col < tcols && tt >= s &&
+                index_ok(blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s) < d.nd, &d.ctl->status)) {
                 ev[u] = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
                 x1v[u] = xsrc[ev[u]];
                 xav[u] = drift ? d.x0[ev[u]] : x1v[u];
@@ -404,8 +406,9 @@ __device__ __forceinline__ void y_kernel_tile(const Dev<Real>& d, int tile, cons
     constexpr int kYChunk = y_chunk<Real>();
     if (g < (long long)d.tp * d.n) {    // uniform over the warp
         const int s = int(g / d.n), i = int(g - (long long)s * d.n);
-        const int len = d.tp - s;
-        const long long e0 = blk(d.n, d.tp, s) + (long long)i * len;
+        const int len = index_ok(blk(d.n, d.tp, s) + (long long)(i + 1) * (d.tp - s) <= d.nd, &d.ctl->status)
+                            ? d.tp - s : 0;
+        const long long e0 = blk(d.n, d.tp, s) + (long long)i * (d.tp - s);
         // chunks of kYChunk values per lane, loaded by predicated loads with
         // no loop around them, so each chunk is one memory round trip (an
         // unrolled loop over the row would end in a remainder loop that waits
@@ -620,8 +623,8 @@ __device__ __forceinline__ void z_task(const Dev<Real>& d, int s, const Real* zs
     const bool vanilla = !Reflect && (gate & kGateVanilla);   // as in the y half-step
     const bool drift = Reflect || (gate & kGateDrift);
     double acc[3] = {0.0, 0.0, 0.0};   // |dz|^2, <dx, dz>, drift
-    const int mine = (r1 - r0) * len;
     const long long sbase = base + (long long)r0 * len;
+    const int mine = index_ok(sbase + (long long)(r1 - r0) * len <= d.nd, &d.ctl->status) ? (r1 - r0) * len : 0;
 
     const bool staged = d.zstaged != 0;
     // v(q) = z + r of the slice's element q, in the same arithmetic either way
@@ -906,7 +909,7 @@ __device__ __forceinline__ void upper_kernel_tile(const Dev<Real>& d, int tile, 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double acc[3] = {0.0, 0.0, 0.0};
     double bmax = 0.0;
-    if (s < tlimit) {
+    if (s < tlimit && index_ok(blk(d.n, d.tp, s) + (long long)d.n * (d.tp - s) <= d.nd, &d.ctl->status)) {
         const int len = d.tp - s, valid = tlimit - s;
         const long long base = blk(d.n, d.tp, s);
         for (int i = warp; i < d.n; i += nwarps) {
@@ -981,7 +984,8 @@ __device__ __forceinline__ void lower_kernel_tile(const Dev<Real>& d, int tile, 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int s = s0 + u * nwarps;
-            in[u] = s < rows && lane < tcols && tt >= s;
+            in[u] = s < rows && lane < tcols && tt >= s &&
+                    index_ok(blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s) < d.nd, &d.ctl->status);
             if (in[u]) {
                 const long long e = blk(d.n, d.tp, s) + (long long)item * (d.tp - s) + (tt - s);
                 hv[u] = d.h[e];
@@ -1510,6 +1514,7 @@ __global__ void sum_rows_kernel(const double* __restrict__ partial, int count, d
 
 // reform_pria_run's return value when the wall-clock budget ran out.
 constexpr int kStatusTimeLimit = REFORM_PRIA_STATUS_TIME_LIMIT;
+constexpr int kStatusBounds = REFORM_PRIA_STATUS_BOUNDS;
 
 struct SolverBase {
     // Wall-clock budget of each run, in seconds; < 0: none.  Checked on the
@@ -2115,7 +2120,7 @@ struct Solver final : SolverBase {
         cudaError_t st = start_solve();
         if (st != cudaSuccess) return int(st);
         if (!mirror->terminated && vanilla_phase() && (st = run_vanilla(started, timed_out)) != cudaSuccess)
-            return int(st);
+            return mirror->status == kBoundsStatus ? kStatusBounds : int(st);
         if (timed_out && !mirror->terminated) return kStatusTimeLimit;
         if (!mirror->terminated) {
             for (int kk = 0; kk < 2; ++kk) {
@@ -2146,6 +2151,7 @@ struct Solver final : SolverBase {
         if ((st = cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
             (st = cudaStreamSynchronize(stream)) != cudaSuccess)
             return int(st);
+        if (mirror->status == kBoundsStatus) return kStatusBounds;
         if (mirror->status) return kMegaWaitError;
         return timed_out && !mirror->terminated ? kStatusTimeLimit : 0;
     }
