@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <limits>
+#include <mutex>
 #include <vector>
 
 namespace rb200 {
@@ -255,5 +256,26 @@ __device__ __forceinline__ T clampv(T v, T lo, T hi) {
 }
 
 inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+// A fact the set-up asks the driver for (an occupancy, a kernel attribute, a
+// device attribute), asked once per process and device and then remembered:
+// `query(int*)` runs the first time for the current device.  Each call site
+// passes its own lambda, whose type keys the memo.
+template <class Query>
+cudaError_t once_per_device(int* out, Query query) {
+    static std::mutex mu;
+    static int value[64];
+    static bool known[64] = {};
+    int dev = 0;
+    RB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!known[dev]) {
+        RB_CUDA_TRY(query(&value[dev]));
+        known[dev] = true;
+    }
+    *out = value[dev];
+    return cudaSuccess;
+}
 
 }  // namespace rb200

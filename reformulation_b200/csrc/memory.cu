@@ -70,6 +70,33 @@ void pinned_put(void* slot) {
     slab_free.push_back(int((static_cast<char*>(slot) - slab_base) / kSlot));
 }
 
+namespace {
+std::mutex streams_mu;
+std::vector<cudaStream_t> idle_streams[64];
+}  // namespace
+
+cudaError_t stream_get(cudaStream_t* out, int* device) {
+    int dev = 0;
+    RB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    *device = dev;
+    {
+        std::lock_guard<std::mutex> lock(streams_mu);
+        if (!idle_streams[dev].empty()) {
+            *out = idle_streams[dev].back();
+            idle_streams[dev].pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaStreamCreateWithFlags(out, cudaStreamNonBlocking);
+}
+
+void stream_put(cudaStream_t s, int device) {
+    if (!s || device < 0 || device >= 64) return;
+    std::lock_guard<std::mutex> lock(streams_mu);
+    idle_streams[device].push_back(s);
+}
+
 }  // namespace rb200
 
 // --- staged host-to-device copies ---------------------------------------------

@@ -18,6 +18,13 @@ cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 void* pinned_get();          // a 256-byte pinned slot, or nullptr
 void pinned_put(void* slot);
 
+// A non-blocking stream of the current device (*device receives it) from a
+// library-owned pool, created on first need; stream_put returns it, idle (the
+// caller has synchronised it), for the next solver.  A one-shot solve then
+// pays no stream creation or destruction.
+cudaError_t stream_get(cudaStream_t* out, int* device);
+void stream_put(cudaStream_t s, int device);
+
 // Host-to-device copies of caller (pageable) memory through a library-owned
 // pinned staging ring: host threads fill one slot while the copy engine drains
 // the other, so the copy runs at the pinned rate instead of the driver's

@@ -76,6 +76,7 @@ constexpr int kEdgeSums = 5;     // sum |y1-y2|^2, <S(x1-x2), y1-y2>, sum |y1-y0
                                  // upper edge term at bx, sum of covering by_1
 constexpr int kCheckBlock = 256;
 constexpr int kPrepBlocks = 296; // fixed grid of the preprocessing reduction
+constexpr int64_t kHostCheckEdges = 16384;   // up to this many edges the set-up checks the input on the host
 
 // Scalar state of the solve (StepArguments' scalars, solver.py:229-256),
 // resident on the device.
@@ -690,6 +691,17 @@ __device__ __forceinline__ bool mega_block_body(const Dev<Real>& d, const Params
     return true;
 }
 
+// CTAs of kBlock threads of `fn` the current device holds at once.
+template <class Fn>
+cudaError_t grid_capacity(Fn fn, int* out) {
+    int dev = 0, sms = 0, per_sm = 0;
+    RB_CUDA_TRY(cudaGetDevice(&dev));
+    RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+    *out = sms * per_sm;
+    return cudaSuccess;
+}
+
 // The push layout only (the slot-1 pull layout is for edge arrays beyond L2).
 template <class Real, bool Wide>
 __global__ void __launch_bounds__(kBlock, 1)
@@ -1260,6 +1272,7 @@ struct Solver final : SolverBase {
     PraqParameters p{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    int stream_dev = -1;   // the device of an owned stream (from the library's stream pool)
     PoolBuf<int> row_ptr, col_ptr, colidx, colpos, perm;
     PoolBuf<int2> ends;
     PoolBuf<Real> w, diag, deg, x1, x2, x0, r, pred, pred1, u0, u2s, u2s1;
@@ -1311,7 +1324,7 @@ struct Solver final : SolverBase {
         warm_x.release(); warm_y.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
-        if (own_stream && stream) cudaStreamDestroy(stream);
+        if (own_stream && stream) stream_put(stream, stream_dev);
     }
 
     // Lay the instance out on the device.  Returns 0, PRAQ_ERROR_INSTANCE or
@@ -1320,8 +1333,7 @@ struct Solver final : SolverBase {
         if (s) {
             stream = s;
         } else {
-            if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
-                return PRAQ_ERROR_CUDA;
+            if (stream_get(&stream, &stream_dev) != cudaSuccess) return PRAQ_ERROR_CUDA;
             own_stream = true;
         }
         mirror = static_cast<Control*>(pinned_get());
@@ -1334,12 +1346,18 @@ struct Solver final : SolverBase {
         // The wide gather halves a warp's chain of dependent loads but takes
         // twice the registers: it wins while the node grid is one wave of it.
         {
-            int dev = 0, sms = 0, per_sm = 0;
-            if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, node_kernel<Real, true, false, true>,
-                                                              kBlock, 0))
-                return PRAQ_ERROR_CUDA;
-            wide = kGather == 1 || (kGather == 2 && nb_node <= sms * per_sm);
+            int waves = 0;   // CTAs of the wide node kernel one wave holds
+            const cudaError_t st = once_per_device(&waves, [](int* v) {
+                int dev = 0, sms = 0, per_sm = 0;
+                RB_CUDA_TRY(cudaGetDevice(&dev));
+                RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+                RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, node_kernel<Real, true, false, true>,
+                                                                          kBlock, 0));
+                *v = sms * per_sm;
+                return cudaSuccess;
+            });
+            if (st != cudaSuccess) return PRAQ_ERROR_CUDA;
+            wide = kGather == 1 || (kGather == 2 && nb_node <= waves);
         }
         for (auto* b : {&x1, &x2, &x0, &r})
             if (b->alloc(n, stream)) return PRAQ_ERROR_CUDA;
@@ -1384,25 +1402,31 @@ struct Solver final : SolverBase {
         mega_grid = 0;
         if (!allow_mega) return cudaSuccess;
         if (!pull) {
-            int dev = 0, sms = 0, per_sm = 0;
-            auto fn = wide ? mega_block_kernel<Real, true> : mega_block_kernel<Real, false>;
-            RB_CUDA_TRY(cudaGetDevice(&dev));
-            RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+            // resident CTAs of each grid form, once per process and device
+            // (one lambda per kernel: the lambda's type keys the memo)
+            int cap = 0;
+            if (wide) {
+                RB_CUDA_TRY(once_per_device(&cap, [](int* v) { return grid_capacity(mega_block_kernel<Real, true>, v); }));
+            } else {
+                RB_CUDA_TRY(once_per_device(&cap, [](int* v) { return grid_capacity(mega_block_kernel<Real, false>, v); }));
+            }
             // no phase has more tiles than this: more CTAs would only wait
-            mega_grid = int(std::min<long long>((long long)per_sm * sms, std::max(nb_node, m ? nb_edge : 1)));
+            mega_grid = int(std::min<long long>(cap, std::max(nb_node, m ? nb_edge : 1)));
             // the single-CTA form: the instance in the shared memory its
-            // static arrays leave
-            auto tfn = tiny_solve_kernel<Real>;
-            cudaFuncAttributes fa{};
-            int optin = 0;
-            RB_CUDA_TRY(cudaFuncGetAttributes(&fa, tfn));
-            RB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            const size_t room = size_t(optin) > fa.sharedSizeBytes ? size_t(optin) - fa.sharedSizeBytes : 0;
+            // static arrays leave (the kernel's limit raised to it once)
+            int room = 0;
+            RB_CUDA_TRY(once_per_device(&room, [](int* v) {
+                int dev = 0, optin = 0;
+                cudaFuncAttributes fa{};
+                RB_CUDA_TRY(cudaGetDevice(&dev));
+                RB_CUDA_TRY(cudaFuncGetAttributes(&fa, tiny_solve_kernel<Real>));
+                RB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+                *v = optin > int(fa.sharedSizeBytes) ? optin - int(fa.sharedSizeBytes) : 0;
+                return cudaFuncSetAttribute(tiny_solve_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, *v);
+            }));
             tiny_smem = tiny_layout(n, m, nb_node, nb_edge, int(sizeof(Real))).total;
             // check_body's row reductions keep the 256-thread order up to 256 rows
-            tiny_fits = tiny_smem <= room && nb_node <= kBlock && nb_edge <= kBlock;
-            if (tiny_fits) RB_CUDA_TRY(cudaFuncSetAttribute(tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(room)));
+            tiny_fits = tiny_smem <= size_t(room) && nb_node <= kBlock && nb_edge <= kBlock;
         }
         // REFORM_PRAQ_MEGA=0|1 sets the initial mode (tests, measurements);
         // REFORM_PRAQ_MEGA_PHANTOM=k makes every barrier wait for k CTAs that
@@ -1521,12 +1545,23 @@ struct Solver final : SolverBase {
         prep_scan_kernel<<<kPrepBlocks, kBlock, 0, stream>>>(n, m, rows.ptr, cols.ptr, vals.ptr, dg.ptr,
                                                             krow.ptr, kcol.ptr, flags.ptr, part.ptr);
         prep_scale_kernel<<<1, kBlock, 0, stream>>>(part.ptr, kPrepBlocks, scale.ptr);
-        int* hflags = reinterpret_cast<int*>(mirror);   // the pinned slot, before it is a mirror
-        *hflags = 0;
-        if (cudaMemcpyAsync(hflags, flags.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream) ||
-            cudaStreamSynchronize(stream))
-            return PRAQ_ERROR_CUDA;
-        const int fl = *hflags;
+        int fl = 0;
+        if (m <= kHostCheckEdges) {
+            // a small instance: the same two facts from the caller's arrays on
+            // the host, instead of a round trip that waits for the device
+            for (int64_t e = 0; e < m; ++e) {
+                const int64_t i = in.rows[e], j = in.cols[e];
+                if (i < 0 || i >= n || j < 0 || j >= n || i == j) fl |= 1;
+                if (e > 0 && in.rows[e - 1] > i) fl |= 2;
+            }
+        } else {
+            int* hflags = reinterpret_cast<int*>(mirror);   // the pinned slot, before it is a mirror
+            *hflags = 0;
+            if (cudaMemcpyAsync(hflags, flags.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream) ||
+                cudaStreamSynchronize(stream))
+                return PRAQ_ERROR_CUDA;
+            fl = *hflags;
+        }
         if (fl & 1) return PRAQ_ERROR_INSTANCE;
         if (ends.alloc(m, stream) || w.alloc(m, stream) || first.alloc(m, stream) ||
             second.alloc(m, stream) || sidx.alloc(m, stream) || row_ptr.alloc(size_t(n) + 1, stream) ||
@@ -1690,8 +1725,13 @@ struct Solver final : SolverBase {
         if (env && !std::strcmp(env, "push")) return false;
         if (env && !std::strcmp(env, "pull")) return true;
         if (kPull != 2) return kPull == 1;
-        int dev = 0, l2 = 0;
-        if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev)) return false;
+        int l2 = 0;
+        if (once_per_device(&l2, [](int* v) {
+                int dev = 0;
+                RB_CUDA_TRY(cudaGetDevice(&dev));
+                return cudaDeviceGetAttribute(v, cudaDevAttrL2CacheSize, dev);
+            }) != cudaSuccess)
+            return false;
         return double(m_) * (12.0 + 4.0 * sizeof(Real)) > 2.0 * double(l2);
     }
 

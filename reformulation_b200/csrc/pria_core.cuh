@@ -1542,6 +1542,7 @@ struct Solver final : SolverBase {
     Params prm{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    int stream_dev = -1;   // the device of an owned stream (from the library's stream pool)
     PoolBuf<Real> h, k, xh, x0, r, yh, y0, zh, z0, x2s, dxs, y2s, z2s;
     PoolBuf<double> px, py, pyz, pup, plo, final_up, thx, thy, thz;
     PoolBuf<double> warm[3];   // dense warm start (FP64), optional
@@ -1594,7 +1595,7 @@ struct Solver final : SolverBase {
         ctl.release();
         if (stream) cudaStreamSynchronize(stream);
         pinned_put(mirror);
-        if (own_stream && stream) cudaStreamDestroy(stream);
+        if (own_stream && stream) stream_put(stream, stream_dev);
     }
 
     cudaError_t begin(int64_t n_, int64_t t_, cudaStream_t s) {
@@ -1606,7 +1607,7 @@ struct Solver final : SolverBase {
         if (s) {
             stream = s;
         } else {
-            RB_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            RB_CUDA_TRY(stream_get(&stream, &stream_dev));
             own_stream = true;
         }
         mirror = static_cast<Control*>(pinned_get());
@@ -1781,9 +1782,7 @@ struct Solver final : SolverBase {
             RB_CUDA_TRY(cudaGetDevice(&dev));
             RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             for (auto fn : {mega_block_kernel<Real, false>, mega_block_kernel<Real, true>}) {
-                int k = 0;
-                RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 int(kMegaSmemLimit)));
+                int k = 0;   // (their shared-memory limit is set with the others, set_attributes)
                 RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, fn, kMegaThreads, mega_smem));
                 per_sm = std::min(per_sm, k);
             }
@@ -1838,12 +1837,12 @@ struct Solver final : SolverBase {
     // never to this instance's own need: a later, smaller instance must not
     // lower the limit under an earlier, larger one.
     template <int TW, bool R, bool C>
-    cudaError_t x_attr() {
+    static cudaError_t x_attr() {
         return cudaFuncSetAttribute(x_kernel<Real, TW, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(x_smem_limit()));
     }
     template <bool R, bool C>
-    cudaError_t yz_attr() {
+    static cudaError_t yz_attr() {
         RB_CUDA_TRY(cudaFuncSetAttribute(y_kernel<Real, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(y_smem_limit())));
         for (auto fn : {z_entry<Real, z_threads<Real>(), R, C, false>(), z_entry<Real, z_threads<Real>(), R, C, true>()}) {
@@ -1854,19 +1853,23 @@ struct Solver final : SolverBase {
     }
     cudaError_t set_attributes() {
         if (x_smem > x_smem_limit()) return cudaErrorInvalidValue;
-        RB_CUDA_TRY((x_attr<kXTile, true, false>()));
-        RB_CUDA_TRY((x_attr<kXTile, true, true>()));
-        RB_CUDA_TRY((x_attr<kXTile, false, true>()));
-        RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, kXTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(x_smem_limit())));
-        RB_CUDA_TRY((yz_attr<true, false>()));
-        RB_CUDA_TRY((yz_attr<true, true>()));
-        RB_CUDA_TRY((yz_attr<false, true>()));
-        if (vanilla_phase()) {
+        int done = 0;   // the limits are the kernels': set once per process and device
+        return once_per_device(&done, [](int* v) {
+            RB_CUDA_TRY((x_attr<kXTile, true, false>()));
+            RB_CUDA_TRY((x_attr<kXTile, true, true>()));
+            RB_CUDA_TRY((x_attr<kXTile, false, true>()));
+            RB_CUDA_TRY(cudaFuncSetAttribute(project_x_kernel<Real, kXTile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(x_smem_limit())));
+            RB_CUDA_TRY((yz_attr<true, false>()));
+            RB_CUDA_TRY((yz_attr<true, true>()));
+            RB_CUDA_TRY((yz_attr<false, true>()));
             RB_CUDA_TRY((x_attr<kXTile, false, false>()));
             RB_CUDA_TRY((yz_attr<false, false>()));
-        }
-        return cudaSuccess;
+            for (auto fn : {mega_block_kernel<Real, false>, mega_block_kernel<Real, true>})
+                RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMegaSmemLimit)));
+            *v = 1;
+            return cudaSuccess;
+        });
     }
 
     // Plain PDHG: the whole solve without Halpern, or warm_steps check blocks
