@@ -1612,6 +1612,7 @@ struct Solver final : SolverBase {
         }
         mirror = static_cast<Control*>(pinned_get());
         if (!mirror) return cudaErrorMemoryAllocation;
+        std::memset(static_cast<void*>(mirror), 0, sizeof(Control));   // no run yet: no trace, nothing done
         return cudaSuccess;
     }
 
@@ -2006,7 +2007,7 @@ struct Solver final : SolverBase {
     // The last run's records, oldest first: min(written, ring, capacity) of
     // them, the most recent; *total = records written.
     int get_trace(reform_trace_record* out, int capacity, int64_t* total) override {
-        const long long len = mirror->trace_len;
+        const long long len = std::max(0LL, mirror->trace_len);
         if (total) *total = len;
         if (!prm.trace || !out || capacity <= 0) return 0;
         std::vector<reform_trace_record> ring(size_t(prm.trace_cap));

@@ -524,6 +524,7 @@ def test_convergence_trace_ring_wraps(native):
     inst = qubo_sparse_bernoulli(0, 200, 0.05)
     with DeviceSolver(inst, Library().parameters(tolerance=1e-7, max_iter=100_000)) as dev:
         dev.set_trace(4096)
+        assert len(dev.trace()) == 0                     # no run yet
         dev.run()
         full = dev.trace()
         dev.set_trace(3)
