@@ -1497,6 +1497,7 @@ struct Solver final : SolverBase {
             if (cudaMemcpyAsync(mirror, d.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
                 cudaStreamSynchronize(stream) != cudaSuccess)
                 return PRAQ_ERROR_CUDA;
+            if (mirror->status) return PRAQ_ERROR_CUDA;   // the checked build caught an index
             if (mirror->terminated) break;
             if (time_limit >= 0.0 &&
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() > time_limit) {
