@@ -68,47 +68,68 @@ constexpr int kCounts = kYZ0 + kMaxGroups;
 
 // --- batched kernels: persistent grids over the work tables ---------------
 
+// The persistent grids walk their table (task t, t + stride, ...) with the
+// next task's instance descriptor fetched into the second of two shared
+// slots by cp.async while the current task runs, so no task waits on its
+// descriptor's load: body(descriptor in shared memory, task).
+template <class D>
+__device__ __forceinline__ void desc_fetch(D* dst, const D* src) {
+    static_assert(sizeof(D) % 16 == 0 && alignof(D) >= 16, "descriptors move in 16-byte pieces");
+    constexpr int kPieces = int(sizeof(D) / 16);
+    if (int(threadIdx.x) < kPieces) {
+        const unsigned s = unsigned(__cvta_generic_to_shared(reinterpret_cast<char*>(dst) + 16 * threadIdx.x));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s),
+                     "l"(reinterpret_cast<const char*>(src) + 16 * threadIdx.x)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <class D, class Body>
+__device__ __forceinline__ void walk_tasks(const D* devs, const int2* tasks, int total, int first, int stride,
+                                           D (&slot)[2], Body body) {
+    if (first >= total) return;
+    int2 w = tasks[first];
+    desc_fetch(&slot[0], devs + w.x);
+    int b = 0;
+    for (int t = first; t < total; t += stride, b ^= 1) {
+        const int2 cur = w;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();   // slot b complete for every thread; every thread done with slot b ^ 1
+        if (t + stride < total) {
+            w = tasks[t + stride];
+            desc_fetch(&slot[b ^ 1], devs + w.x);
+        }
+        body(slot[b], cur);
+    }
+}
+
 template <class Real, bool Reflect, bool Check>
 __global__ void __launch_bounds__(praq::kBlock)
 bq_node(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
-    __shared__ praq::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ praq::Dev<Real> slot[2];
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const praq::Dev<Real>& sd, int2 w) {
         praq::node_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? sd.pred : sd.u2s,
                                                      Reflect ? sd.pred1 : sd.u2s1, step, 0, gate);
-    }
+    });
 }
 
 template <class Real, bool Reflect, bool Check>
 __global__ void __launch_bounds__(praq::kBlock)
 bq_edge(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
-    __shared__ praq::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ praq::Dev<Real> slot[2];
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const praq::Dev<Real>& sd, int2 w) {
         praq::edge_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? nullptr : sd.u2s, step, 0, gate);
-    }
+    });
 }
 
 template <class Real>
 __global__ void __launch_bounds__(praq::kBlock)
 bq_lower(const praq::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count) {
-    __shared__ praq::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ praq::Dev<Real> slot[2];
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const praq::Dev<Real>& sd, int2 w) {
         praq::lower_kernel_tile<Real>(sd, w.y, sd.u2s, sd.u2s1);
-    }
+    });
 }
 
 template <class Real>
@@ -128,34 +149,24 @@ bq_check(const praq::Dev<Real>* devs, const QMeta* metas, const int* __restrict_
 template <class Real, int TW, bool Reflect, bool Check>
 __global__ void __launch_bounds__(pria::kXThreads)
 bj_x(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
-    __shared__ pria::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ pria::Dev<Real> slot[2];
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const pria::Dev<Real>& sd, int2 w) {
         if (Reflect)
             pria::x_kernel_tile<Real, TW, Reflect, Check>(sd, w.y, sd.xh, sd.yh, sd.zh, step, gate);
         else
             pria::x_kernel_tile<Real, TW, Reflect, Check>(sd, w.y, sd.x2s, sd.y2s, sd.z2s, step, gate);
-    }
+    });
 }
 
 template <class Real, bool Reflect, bool Check>
 __global__ void __launch_bounds__(pria::kYThreads)
 bj_y(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count, int step, int gate) {
-    __shared__ pria::Dev<Real> sd;
+    __shared__ pria::Dev<Real> slot[2];
     extern __shared__ __align__(16) unsigned char smem_raw[];   // kYThreads / 32 rows of kMaxPeriods
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const pria::Dev<Real>& sd, int2 w) {
         pria::y_kernel_tile<Real, Reflect, Check>(sd, w.y, Reflect ? sd.yh : sd.y2s, step, gate,
                                                   reinterpret_cast<Real*>(smem_raw), pria::kMaxPeriods);
-    }
+    });
 }
 
 // Persistent clusters: cluster c takes tasks c, c + clusters, ...; every CTA
@@ -164,44 +175,29 @@ template <class Real, int kThreads, bool Reflect, bool Check>
 __global__ void __launch_bounds__(kThreads)
 bj_z(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count, int csize, int step,
      int gate) {
-    __shared__ pria::Dev<Real> sd;
-    const int total = *count;
+    __shared__ pria::Dev<Real> slot[2];
     const int nclusters = int(gridDim.x) / csize;
-    for (int t = int(blockIdx.x) / csize; t < total; t += nclusters) {
-        const int2 w = tasks[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    walk_tasks(devs, tasks, *count, int(blockIdx.x) / csize, nclusters, slot, [&](const pria::Dev<Real>& sd, int2 w) {
         pria::z_task<Real, kThreads, Reflect, Check>(sd, w.y, Reflect ? sd.zh : sd.z2s, step, gate);
-    }
+    });
 }
 
 template <class Real>
 __global__ void __launch_bounds__(pria::kAuxThreads)
 bj_upper(const pria::Dev<Real>* devs, const int2* __restrict__ tasks, const int* count) {
-    __shared__ pria::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tasks[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ pria::Dev<Real> slot[2];
+    walk_tasks(devs, tasks, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const pria::Dev<Real>& sd, int2 w) {
         pria::upper_kernel_tile<Real>(sd, w.y, sd.x2s, sd.tp, 0);
-    }
+    });
 }
 
 template <class Real>
 __global__ void __launch_bounds__(pria::kAuxThreads)
 bj_lower(const pria::Dev<Real>* devs, const int2* __restrict__ tiles, const int* count) {
-    __shared__ pria::Dev<Real> sd;
-    const int total = *count;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int2 w = tiles[t];
-        __syncthreads();
-        if (threadIdx.x == 0) sd = devs[w.x];
-        __syncthreads();
+    __shared__ pria::Dev<Real> slot[2];
+    walk_tasks(devs, tiles, *count, int(blockIdx.x), int(gridDim.x), slot, [&](const pria::Dev<Real>& sd, int2 w) {
         pria::lower_kernel_tile<Real>(sd, w.y, sd.y2s, sd.z2s);
-    }
+    });
 }
 
 template <class Real>

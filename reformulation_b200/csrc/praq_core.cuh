@@ -102,7 +102,7 @@ struct Params {
 };
 
 template <class Real>
-struct Dev {
+struct alignas(16) Dev {   // (16-byte aligned: the batched engine copies descriptors in 16-byte pieces)
     int n, m;
     const int* row_ptr;    // [n+1] first-end runs in sorted edge order
     const int* col_ptr;    // [n+1] second-end runs in second-end order

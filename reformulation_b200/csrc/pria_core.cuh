@@ -135,7 +135,7 @@ __host__ __device__ __forceinline__ long long blk(int n, int tp, int s) {
 }
 
 template <class Real>
-struct Dev {
+struct alignas(16) Dev {   // (16-byte aligned: the batched engine copies descriptors in 16-byte pieces)
     int n, t, tp, ntc, ntc_low, csize;
     int zpair;               // 1: the solver's z launch takes period blocks in pairs (s, Tp - 1 - s)
                              //    (z_task_pair); 0: one block per cluster (z_task, which the
