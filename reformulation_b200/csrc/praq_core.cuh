@@ -71,6 +71,20 @@ constexpr int kBlock = 256;
 #define RB200_PRAQ_EDGES_PER_THREAD 4   // compile-time tunable (sweeps build with -D)
 #endif
 constexpr int kEdgesPerThread = RB200_PRAQ_EDGES_PER_THREAD;
+// The steps without check sums have no per-tile results, so their edge grid
+// may be cut differently from the check steps': FP32 iterates in the push
+// layout (edge arrays in L2) take two edges a thread, twice the CTAs, which
+// measured 2.6 % faster on the whole solve at n = 1e5, m = 1e6 than four (one:
+// 0.6 %); FP64 iterates there, and the pull layout (edge arrays streamed from
+// HBM), keep four (two: FP64 3 % slower at n = 1e5; FP32 1.3 % slower at
+// n = 2e6, m = 2e7).
+#ifndef RB200_PRAQ_PUSH_EDGES_PER_THREAD_F32
+#define RB200_PRAQ_PUSH_EDGES_PER_THREAD_F32 2
+#endif
+template <class Real, bool Pull>
+constexpr int plain_edges_per_thread() {
+    return !Pull && sizeof(Real) == 4 ? RB200_PRAQ_PUSH_EDGES_PER_THREAD_F32 : kEdgesPerThread;
+}
 constexpr int kNodeSums = 3;     // sum deg (x1-x2)^2, sum deg (x1-x0)^2, sum d . bx
 constexpr int kEdgeSums = 5;     // sum |y1-y2|^2, <S(x1-x2), y1-y2>, sum |y1-y0|^2,
                                  // upper edge term at bx, sum of covering by_1
@@ -405,20 +419,20 @@ node_kernel(Dev<Real> d, const Real* __restrict__ ys, const Real* __restrict__ y
 // one-coordinate form, plus the prediction of the next step's combined dual.
 // Each thread takes kEdgesPerThread edges a block-stride apart, so all their
 // loads are in flight together.
-template <class Real, bool Reflect, bool Check, bool Pull = false>
+template <class Real, bool Reflect, bool Check, bool Pull = false, int EPT = kEdgesPerThread>
 __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, const Real* ysrc, int step, int bounds_at_1, int gate) {
     const Control* c = d.ctl;
     if (skip(c, gate)) return;
     __shared__ double scratch[kEdgeSums * 32];
-    const int base = tile * (kBlock * kEdgesPerThread) + threadIdx.x;
+    const int base = tile * (kBlock * EPT) + threadIdx.x;
     const Real hs = Real(0.5 * kEta * c->omega);
     const double kn = Reflect ? double(c->restart_iter + step + 2) : 1.0;
     const Real lwn = Real(kn / (kn + 1.0)), rwn = Real(1.0 / (kn + 1.0));
-    int2 ij[kEdgesPerThread];
-    Real sw[kEdgesPerThread], u1[kEdgesPerThread], u0[kEdgesPerThread];
-    int at1[kEdgesPerThread];   // where slot 1 goes: the edge (pull) or its second-end position (push)
+    int2 ij[EPT];
+    Real sw[EPT], u1[EPT], u0[EPT];
+    int at1[EPT];   // where slot 1 goes: the edge (pull) or its second-end position (push)
 #pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
+    for (int t = 0; t < EPT; ++t) {
         const int e = base + t * kBlock;
         if (e < d.m) {
             ij[t] = d.ends[e];
@@ -428,9 +442,9 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
             at1[t] = Pull ? e : d.colpos[e];
         }
     }
-    Real ri[kEdgesPerThread], rj[kEdgesPerThread];
+    Real ri[EPT], rj[EPT];
 #pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
+    for (int t = 0; t < EPT; ++t) {
         if (base + t * kBlock < d.m) {
             const bool ok = index_ok(unsigned(ij[t].x) < unsigned(d.n) && unsigned(ij[t].y) < unsigned(d.n),
                                      &d.ctl->status);
@@ -441,7 +455,7 @@ __device__ __forceinline__ void edge_kernel_tile(const Dev<Real>& d, int tile, c
     }
     double acc[kEdgeSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int t = 0; t < kEdgesPerThread; ++t) {
+    for (int t = 0; t < EPT; ++t) {
         const int e = base + t * kBlock;
         if (e >= d.m) continue;
         const bool cov = sw[t] > Real(0);
@@ -486,6 +500,16 @@ edge_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) 
     pdl_wait();
     pdl_launch_dependents();
     edge_kernel_tile<Real, Reflect, Check, Pull>(d, blockIdx.x, ysrc, step, bounds_at_1, gate);
+}
+
+// The reflected step without check sums, on its own grid (tiles of kBlock *
+// plain_edges_per_thread<Real, Pull>() edges).
+template <class Real, bool Pull = false>
+__global__ void __launch_bounds__(kBlock)
+edge_plain_kernel(Dev<Real> d, const Real* ysrc, int step, int bounds_at_1, int gate) {
+    pdl_wait();
+    pdl_launch_dependents();
+    edge_kernel_tile<Real, true, false, Pull, plain_edges_per_thread<Real, Pull>()>(d, blockIdx.x, ysrc, step, bounds_at_1, gate);
 }
 
 // The node part of the lower bound, sum_i min(d_i - (S^T y)_i, 0), at the
@@ -1281,7 +1305,7 @@ struct Solver final : SolverBase {
     PoolBuf<Control> ctl;
     Control* mirror = nullptr;   // pinned host copy of the control block
     Dev<Real> d{};
-    int nb_node = 1, nb_edge = 1;
+    int nb_node = 1, nb_edge = 1, nb_edge_push = 1, nb_edge_pull = 1;
     bool wide = false;   // node gather of both runs at once (warp_runs2)
     bool pull = false;   // slot-1 layout (see the layout notes at the top)
     bool allow_pull = true;   // false: always push (the batched engine's kernels)
@@ -1344,6 +1368,8 @@ struct Solver final : SolverBase {
         if (st) return st;
         nb_node = ceil_div(n, kBlock);   // one node per thread
         nb_edge = std::max(1, ceil_div(m, kBlock * kEdgesPerThread));
+        nb_edge_push = std::max(1, ceil_div(m, kBlock * plain_edges_per_thread<Real, false>()));
+        nb_edge_pull = std::max(1, ceil_div(m, kBlock * plain_edges_per_thread<Real, true>()));
         // The wide gather halves a warp's chain of dependent loads but takes
         // twice the registers: it wins while the node grid is one wave of it.
         {
@@ -1656,7 +1682,7 @@ struct Solver final : SolverBase {
         for (int s = 0; s < op; ++s) {
             if (s + 1 < op) {
                 RB_TIMED(0, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, false, W, P>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.pred1, s, 0, 0)));
-                if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, false, P>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
+                if (m) RB_TIMED(1, RB_CUDA_TRY(launch_pdl(edge_plain_kernel<Real, P>, P ? nb_edge_pull : nb_edge_push, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));
             } else {
                 RB_TIMED(2, RB_CUDA_TRY(launch_pdl(node_kernel<Real, true, true, W, P>, nb_node, kBlock, stream, d, (const Real*)d.pred, (const Real*)d.pred1, s, 0, 0)));
                 if (m) RB_TIMED(3, RB_CUDA_TRY(launch_pdl(edge_kernel<Real, true, true, P>, nb_edge, kBlock, stream, d, (const Real*)nullptr, s, 0, 0)));

@@ -253,6 +253,43 @@ def test_edgeless_instance_terminates(lib):
 
 
 @pytest.mark.parametrize("use_float32", [0, 1])
+def test_upload_modes_agree(lib, monkeypatch, use_float32):
+    """The instance arrays cross to the device by the driver's copy (the
+    default) or through the library's pinned staging ring ("staged"): the
+    same layout, so the same solve bit for bit, sorted or shuffled; and both
+    reject an end out of range or a self-loop anywhere in the arrays.  25k
+    edges: above the size whose flags the set-up finds on the host, so the
+    device's scan raises them."""
+    base = random_qubo(21, 5000, 0.002)
+    assert base.edges > 16384
+    rng = np.random.default_rng(3)
+    order = rng.permutation(base.edges)
+    flip = rng.random(base.edges) < 0.5
+    rows, cols = base.rows[order].copy(), base.cols[order].copy()
+    rows[flip], cols[flip] = cols[flip], rows[flip].copy()
+    shuffled = QuboInstance("s", "s", base.n, base.diag, rows, cols, base.vals[order])
+    p = lib.parameters(tolerance=1e-4 if use_float32 else 1e-7, use_float32=use_float32)
+    out = {}
+    for mode in ("direct", "staged"):
+        monkeypatch.setenv("REFORM_PRAQ_UPLOAD", mode)
+        out[mode] = [lib.solve(inst, p) for inst in (base, shuffled)]
+        for k, (where, value) in enumerate(((base.edges - 1, base.n), (12345, None), (0, -1),
+                                             (base.edges // 2, 1 << 32))):
+            bad = QuboInstance("b", "b", base.n, base.diag, base.rows.copy(), base.cols.copy(), base.vals)
+            if value is None:
+                bad.cols[where] = bad.rows[where]    # a self-loop
+            elif k % 2:
+                bad.rows[where] = value
+            else:
+                bad.cols[where] = value
+            assert lib.solve(bad, p).status == -2, (mode, where, value)
+    for a, b in zip(out["direct"], out["staged"]):
+        assert a.status == b.status == 0
+        assert (a.iterations, a.lower, a.upper) == (b.iterations, b.lower, b.upper)
+        assert np.array_equal(a.x, b.x)
+
+
+@pytest.mark.parametrize("use_float32", [0, 1])
 def test_slot1_layouts_agree(native, oracle_lib, monkeypatch, use_float32):
     """The two slot-1 layouts (push: scattered by the edge kernel; pull:
     gathered by the node kernel through the second-end index) add the same
