@@ -210,7 +210,84 @@ cudaError_t staged(char* dst, size_t bytes, size_t unit, cudaStream_t stream, Fi
     return cudaSuccess;
 }
 
+// Copies `bytes` of device memory at src back in chunks through the ring:
+// chunk c + 1 is copied while drain(first_unit, units, slot) hands chunk c on,
+// split over the host threads (on the calling thread alone for small chunks).
+template <class Drain>
+cudaError_t staged_back(const char* src, size_t bytes, size_t unit, cudaStream_t stream, Drain drain) {
+    if (!bytes) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(stage_mu);
+    int dev = 0;
+    RB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!stage_ring && cudaHostAlloc(reinterpret_cast<void**>(&stage_ring), 2 * kStageBytes,
+                                     cudaHostAllocPortable) != cudaSuccess) {
+        stage_ring = nullptr;
+        (void)cudaGetLastError();
+        return cudaErrorMemoryAllocation;
+    }
+    for (auto& ev : stage_done[dev])
+        if (!ev) RB_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const size_t chunk = kStageBytes / unit * unit;
+    const size_t chunks = (bytes + chunk - 1) / chunk;
+    auto issue = [&](size_t c) -> cudaError_t {
+        const int slot = int(c & 1);
+        if (stage_dev[slot] >= 0)   // the slot's last copy, from whichever device, is done
+            RB_CUDA_TRY(cudaEventSynchronize(stage_done[stage_dev[slot]][slot]));
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        RB_CUDA_TRY(cudaMemcpyAsync(stage_ring + size_t(slot) * kStageBytes, src + off, len,
+                                    cudaMemcpyDeviceToHost, stream));
+        RB_CUDA_TRY(cudaEventRecord(stage_done[dev][slot], stream));
+        stage_dev[slot] = dev;
+        return cudaSuccess;
+    };
+    RB_CUDA_TRY(issue(0));
+    HostThreads& pool = host_threads();
+    constexpr size_t kAloneUnits = size_t(1) << 15;   // below this a chunk is drained on one thread
+    for (size_t c = 0; c < chunks; ++c) {
+        if (c + 1 < chunks) RB_CUDA_TRY(issue(c + 1));
+        const int slot = int(c & 1);
+        RB_CUDA_TRY(cudaEventSynchronize(stage_done[dev][slot]));
+        const char* buf = stage_ring + size_t(slot) * kStageBytes;
+        const size_t first = c * chunk / unit, units = std::min(chunk, bytes - c * chunk) / unit;
+        if (units < kAloneUnits) {
+            drain(first, units, buf);
+            continue;
+        }
+        const size_t parts = size_t(pool.size());
+        pool.parallel([&](int k) {
+            const size_t a = units * size_t(k) / parts, b = units * size_t(k + 1) / parts;
+            if (b > a) drain(first + a, b - a, buf + a * unit);
+        });
+    }
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t download_as_double(double* dst, const T* src, size_t count, cudaStream_t stream) {
+    return staged_back(reinterpret_cast<const char*>(src), sizeof(T) * count, sizeof(T), stream,
+                       [dst](size_t first, size_t units, const char* from) {
+                           const T* v = reinterpret_cast<const T*>(from);
+                           double* out = dst + first;
+                           for (size_t k = 0; k < units; ++k) out[k] = double(v[k]);
+                       });
+}
+
 }  // namespace
+
+cudaError_t staged_download_as_double(double* dst, const float* src, size_t count, cudaStream_t stream) {
+    return download_as_double(dst, src, count, stream);
+}
+
+cudaError_t staged_download_as_double(double* dst, const double* src, size_t count, cudaStream_t stream) {
+    return download_as_double(dst, src, count, stream);
+}
+
+cudaError_t staged_download(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    char* out = static_cast<char*>(dst);
+    return staged_back(static_cast<const char*>(src), bytes, 1, stream,
+                       [out](size_t first, size_t len, const char* from) { std::memcpy(out + first, from, len); });
+}
 
 cudaError_t staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
     const char* s = static_cast<const char*>(src);

@@ -33,6 +33,19 @@ void stream_put(cudaStream_t s, int device);
 // threads take turns.
 cudaError_t staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t stream);
 
+// Device-to-host copy of `count` values into caller (pageable) memory as
+// doubles, through the same pinned ring: the copy engine fills one slot
+// while the host threads widen the other into dst, so the caller's pages are
+// first touched by several threads at once and no host staging vector is
+// allocated.  Returns once dst is complete (the stream is synchronised up to
+// the last chunk's copy).
+cudaError_t staged_download_as_double(double* dst, const float* src, size_t count, cudaStream_t stream);
+cudaError_t staged_download_as_double(double* dst, const double* src, size_t count, cudaStream_t stream);
+// The same for `bytes` copied as they are.  Both return
+// cudaErrorMemoryAllocation, having copied nothing, when no pinned ring can
+// be had.
+cudaError_t staged_download(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+
 template <class T>
 struct PoolBuf {
     T* ptr = nullptr;

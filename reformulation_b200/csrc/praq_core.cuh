@@ -1893,12 +1893,19 @@ struct Solver final : SolverBase {
     int result(double* x, double* y2, PraqResult* res) override {
         const Control c = *mirror;
         if (x) {
-            std::vector<Real> hx(n);
             const Real* src = c.result_slot == 1 ? d.x1 : d.x2;
-            if (cudaMemcpyAsync(hx.data(), src, sizeof(Real) * n, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-                cudaStreamSynchronize(stream) != cudaSuccess)
+            // through the library's pinned ring (no ring to be had: a host
+            // vector and the driver's pageable copy)
+            const cudaError_t st = staged_download_as_double(x, src, size_t(n), stream);
+            if (st == cudaErrorMemoryAllocation) {
+                std::vector<Real> hx(n);
+                if (cudaMemcpyAsync(hx.data(), src, sizeof(Real) * n, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+                    cudaStreamSynchronize(stream) != cudaSuccess)
+                    return PRAQ_ERROR_CUDA;
+                for (int i = 0; i < n; ++i) x[i] = double(hx[i]);
+            } else if (st != cudaSuccess) {
                 return PRAQ_ERROR_CUDA;
-            for (int i = 0; i < n; ++i) x[i] = double(hx[i]);
+            }
         }
         if (y2 && m) {
             std::vector<Real> hu(m), hw(m);
