@@ -2,6 +2,7 @@
 #include "memory.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstdint>
 #include <cstring>
@@ -105,12 +106,17 @@ namespace rb200 {
 namespace {
 
 // A fixed set of host threads that run one job at a time: parallel(f) calls
-// f(k) for k = 0 .. size-1, k = 0 on the calling thread, and returns when all
-// have returned.  Started on first use, joined at exit.
+// f(k) once for every k = 0 .. size-1 and returns when all calls have
+// returned.  The parts are claimed from a counter by the calling thread and
+// by whichever helpers wake while the job is open, so a helper that the
+// system does not schedule in time (other processes on the host) holds
+// nothing up: its parts go to the others, and once every part is claimed the
+// job closes and the caller waits only for the helpers that joined it.
+// Started on first use, joined at exit.
 class HostThreads {
 public:
     explicit HostThreads(int helpers) : helpers_(helpers) {
-        for (int k = 1; k <= helpers_; ++k) threads_.emplace_back([this, k] { loop(k); });
+        for (int k = 1; k <= helpers_; ++k) threads_.emplace_back([this] { loop(); });
     }
     ~HostThreads() {
         {
@@ -125,31 +131,38 @@ public:
         {
             std::lock_guard<std::mutex> lock(mu_);
             job_ = &f;
-            pending_ = helpers_;
+            parts_ = size();
+            next_.store(0, std::memory_order_relaxed);
+            open_ = true;
             ++generation_;
         }
         wake_.notify_all();
-        f(0);
+        run_parts(f);
         std::unique_lock<std::mutex> lock(mu_);
-        done_.wait(lock, [this] { return pending_ == 0; });
+        open_ = false;   // every part is claimed: no helper joins from here on
+        done_.wait(lock, [this] { return active_ == 0; });
         job_ = nullptr;
     }
 
 private:
-    void loop(int k) {
+    void run_parts(const std::function<void(int)>& f) {
+        for (int k; (k = next_.fetch_add(1, std::memory_order_relaxed)) < parts_;) f(k);
+    }
+    void loop() {
         long long seen = 0;
         for (;;) {
             const std::function<void(int)>* f;
             {
                 std::unique_lock<std::mutex> lock(mu_);
-                wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
+                wake_.wait(lock, [&] { return stop_ || (open_ && generation_ != seen); });
                 if (stop_) return;
                 seen = generation_;
                 f = job_;
+                ++active_;
             }
-            (*f)(k);
+            run_parts(*f);
             std::lock_guard<std::mutex> lock(mu_);
-            if (--pending_ == 0) done_.notify_one();
+            if (--active_ == 0) done_.notify_all();
         }
     }
     int helpers_;
@@ -157,8 +170,11 @@ private:
     std::mutex mu_;
     std::condition_variable wake_, done_;
     const std::function<void(int)>* job_ = nullptr;
+    int parts_ = 0;
+    std::atomic<int> next_{0};
     long long generation_ = 0;
-    int pending_ = 0;
+    int active_ = 0;
+    bool open_ = false;
     bool stop_ = false;
 };
 
