@@ -1731,14 +1731,19 @@ struct Solver final : SolverBase {
     }
 
     // Host -> device copy of one of the caller's (pageable) instance arrays:
-    // the driver's own pageable copy, or the library's pinned staging ring
-    // (host threads fill one slot while the copy engine drains the other).
-    // REFORM_PRAQ_UPLOAD=staged|direct in the environment picks one (for
-    // measurements); the default is the driver's copy.
+    // an array of at least kRingUploadBytes goes through the library's pinned
+    // staging ring (host threads fill one slot while the copy engine drains
+    // the other), a smaller one by the driver's own pageable copy, whose
+    // rate varies from host to host (B200 boxes of one pool: 7.7 to 20 GB/s
+    // pageable against 21 to 51 GB/s pinned).  REFORM_PRAQ_UPLOAD=staged|direct
+    // in the environment sends every array one way (for measurements).
+    static constexpr size_t kRingUploadBytes = size_t(1) << 20;
     template <class T>
     cudaError_t upload_input(PoolBuf<T>& b, const T* host, size_t count) {
         const char* env = std::getenv("REFORM_PRAQ_UPLOAD");
-        if (!(env && !std::strcmp(env, "staged"))) return b.upload(host, count, stream);
+        const bool direct = env && !std::strcmp(env, "direct");
+        const bool staged = env && !std::strcmp(env, "staged");
+        if (direct || (!staged && sizeof(T) * count < kRingUploadBytes)) return b.upload(host, count, stream);
         RB_CUDA_TRY(b.alloc(count, stream));
         return staged_upload(b.ptr, host, sizeof(T) * count, stream);
     }
