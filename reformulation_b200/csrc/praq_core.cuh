@@ -631,6 +631,13 @@ check_kernel(Control* c, Params p, const double* __restrict__ scale_ptr,
     check_body(c, p, scale_ptr, pnode, nbn, pedge, nbe, plower, nbl, mode);
 }
 
+// The head of a captured check block: the block's body runs only while the
+// solve has not terminated (a block queued behind the one that ended the
+// solve then costs this one launch instead of its ~37 gated kernels).
+__global__ void block_gate_kernel(const Control* c, cudaGraphConditionalHandle body) {
+    if (threadIdx.x == 0) cudaGraphSetConditional(body, c->terminated ? 0u : 1u);
+}
+
 // ---- the persistent kernel for small instances ----------------------------
 // One cooperative launch runs a whole check block: op_steps steps of the node
 // half and the edge half, the lower-bound pass, the check and the gated
@@ -1314,6 +1321,7 @@ struct Solver final : SolverBase {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
+    bool gated = false;   // the captured block is the conditional (gated) graph
     int status_override = -100;
     int runs = 0;
     // The persistent kernel in place of the graph, in its grid form
@@ -1555,7 +1563,7 @@ struct Solver final : SolverBase {
         if (wide) return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, true>, d, prm, a);
         return cudaLaunchKernelEx(&cfg, mega_block_kernel<Real, false>, d, prm, a);
     }
-    long long block_launches() const { return mega ? 1 : block_nodes; }
+    long long block_launches() const { return mega ? 1 : block_nodes + (exec && gated ? 1 : 0); }
 
     int layout(const PraqInstance& in) {
         n = int(in.n);
@@ -1699,10 +1707,51 @@ struct Solver final : SolverBase {
         return cudaGetLastError();
     }
 
+    // The repeated runs' check block as one graph: block_gate_kernel, then a
+    // conditional node whose body is the captured block, so a block launched
+    // after termination skips its body on the device.  Where the conditional
+    // graph cannot be built, the plain captured block (its kernels gated
+    // one by one).
     cudaError_t capture_block() {
+        gated = capture_gated_block() == cudaSuccess;
+        if (gated) return cudaSuccess;
+        (void)cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
         RB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t st = enqueue_block();
         cudaError_t st2 = cudaStreamEndCapture(stream, &graph);
+        RB_CUDA_TRY(st);
+        RB_CUDA_TRY(st2);
+        return cudaGraphInstantiate(&exec, graph, 0);
+    }
+
+    cudaError_t capture_gated_block() {
+        RB_CUDA_TRY(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle;
+        RB_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t gate;
+        cudaKernelNodeParams kp = {};
+        void* args[2] = {&d.ctl, &handle};
+        kp.func = reinterpret_cast<void*>(block_gate_kernel);
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.kernelParams = args;
+        RB_CUDA_TRY(cudaGraphAddKernelNode(&gate, graph, nullptr, 0, &kp));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cond;
+        RB_CUDA_TRY(cudaGraphAddNode(&cond, graph, &gate, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        RB_CUDA_TRY(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cudaError_t st = enqueue_block();
+        cudaGraph_t captured = nullptr;
+        cudaError_t st2 = cudaStreamEndCapture(stream, &captured);
         RB_CUDA_TRY(st);
         RB_CUDA_TRY(st2);
         return cudaGraphInstantiate(&exec, graph, 0);
@@ -1813,6 +1862,8 @@ struct Solver final : SolverBase {
             int k = 0;
             for (;;) {
                 if (cudaEventSynchronize(done[k]) != cudaSuccess) return PRAQ_ERROR_CUDA;
+                if (mirror->terminated && !mirror->status && exec && gated && !mega)
+                    nlaunch -= block_nodes;   // the block behind it ran its gate alone
                 if (mirror->status || mirror->terminated) break;
                 if (time_limit >= 0.0 &&
                     std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count() >

@@ -253,6 +253,32 @@ def test_edgeless_instance_terminates(lib):
 
 
 @pytest.mark.parametrize("use_float32", [0, 1])
+def test_gated_block_graph(native, use_float32):
+    """A solver's first run launches its kernels one by one; later runs
+    replay the captured check block, a conditional graph whose body runs only
+    while the solve has not terminated.  The results are the first run's bit
+    for bit, and the block queued behind the one that ended the solve runs its
+    gate kernel alone, so a replayed run launches fewer kernels than the first
+    (the same number every time)."""
+    from reformulation_b200.instances import qubo_uniform_edges
+    from reformulation_b200.praq import DeviceSolver, Library
+    inst = qubo_uniform_edges(5, 20000, 200000)
+    p = Library().parameters(tolerance=1e-4 if use_float32 else 1e-7, use_float32=use_float32)
+    runs, launches = [], []
+    with DeviceSolver(inst, p) as dev:
+        dev.set_megakernel(0)
+        for _ in range(3):
+            assert dev.run() == 0
+            runs.append(dev.result(want_x=True, want_dual=True))
+            launches.append(dev.launches())
+    (a, ya), *rest = runs
+    for b, yb in rest:
+        assert (a.iterations, a.lower, a.upper) == (b.iterations, b.lower, b.upper)
+        assert np.array_equal(a.x, b.x) and np.array_equal(ya, yb)
+    assert launches[1] < launches[0] and launches[2] == launches[1], launches
+
+
+@pytest.mark.parametrize("use_float32", [0, 1])
 def test_upload_modes_agree(lib, monkeypatch, use_float32):
     """The instance arrays cross to the device by the driver's copy (the
     default) or through the library's pinned staging ring ("staged"): the
