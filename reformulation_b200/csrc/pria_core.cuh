@@ -1230,6 +1230,13 @@ __device__ __forceinline__ void mega_check(Control* c, const Params& prm, const 
     if (blockIdx.x == 0) check_body(c, prm, px, nbx, py, nby, pyz, nbyz, pup, nbup, plo, nblo, mode);
 }
 
+// The head of a captured check block: the block's body runs only while the
+// solve has not terminated (a block queued behind the one that ended the
+// solve then costs this one launch instead of its gated kernels).
+__global__ void block_gate_kernel(const Control* c, cudaGraphConditionalHandle body) {
+    if (threadIdx.x == 0) cudaGraphSetConditional(body, c->terminated ? 0u : 1u);
+}
+
 // Vanilla: one block of the vanilla phase (enqueue_vanilla_block's steps);
 // otherwise one Halpern check block (enqueue_block's).
 template <class Real, bool Vanilla>
@@ -1556,6 +1563,7 @@ struct Solver final : SolverBase {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};
     long long nlaunch = 0, block_nodes = 0;
+    bool gated = false;   // the captured block is the conditional (gated) graph
     int runs = 0;
     // The persistent kernel (mega_block_kernel) in place of the graph: chosen
     // at set-up (mode -1: at most kMegaAutoEntries packed entries), or forced
@@ -1965,7 +1973,19 @@ struct Solver final : SolverBase {
         return cudaGetLastError();
     }
 
+    // The repeated runs' check block as one graph: block_gate_kernel, then a
+    // conditional node whose body is the captured block, so a block launched
+    // after termination skips its body on the device.  Where the conditional
+    // graph cannot be built, the plain captured block (its kernels gated
+    // one by one).
     cudaError_t capture_block() {
+        gated = capture_gated_block() == cudaSuccess;
+        if (gated) return cudaSuccess;
+        (void)cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
         RB_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t st = enqueue_block();
         cudaError_t st2 = cudaStreamEndCapture(stream, &graph);
@@ -1974,8 +1994,37 @@ struct Solver final : SolverBase {
         return cudaGraphInstantiate(&exec, graph, 0);
     }
 
+    cudaError_t capture_gated_block() {
+        RB_CUDA_TRY(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle;
+        RB_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+        cudaGraphNode_t gate;
+        cudaKernelNodeParams kp = {};
+        void* args[2] = {&d.ctl, &handle};
+        kp.func = reinterpret_cast<void*>(block_gate_kernel);
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.kernelParams = args;
+        RB_CUDA_TRY(cudaGraphAddKernelNode(&gate, graph, nullptr, 0, &kp));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cond;
+        RB_CUDA_TRY(cudaGraphAddNode(&cond, graph, &gate, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        RB_CUDA_TRY(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cudaError_t st = enqueue_block();
+        cudaGraph_t captured = nullptr;
+        cudaError_t st2 = cudaStreamEndCapture(stream, &captured);
+        RB_CUDA_TRY(st);
+        RB_CUDA_TRY(st2);
+        return cudaGraphInstantiate(&exec, graph, 0);
+    }
+
     cudaError_t launch_block() { return exec && !mega ? cudaGraphLaunch(exec, stream) : enqueue_block(); }
-    long long block_launches() const { return mega ? 1 : block_nodes; }
+    long long block_launches() const { return mega ? 1 : block_nodes + (exec && gated ? 1 : 0); }
     // the error of a block whose grid barrier ran out (the persistent kernel)
     static constexpr int kMegaWaitError = int(cudaErrorLaunchTimeout);
 
@@ -2135,6 +2184,8 @@ struct Solver final : SolverBase {
             int kk = 0;
             for (;;) {
                 if ((st = cudaEventSynchronize(done[kk])) != cudaSuccess) return int(st);
+                if (mirror->terminated && !mirror->status && exec && gated && !mega)
+                    nlaunch -= block_nodes;   // the block behind it ran its gate alone
                 if (mirror->status || mirror->terminated) break;
                 if (p.verbose)
                     fprintf(stderr, "pria: iter %8lld  primal %.9e  dual %.9e  gap %.3e  omega %.3e\n",

@@ -368,6 +368,27 @@ def _same(a, b):
         assert np.array_equal(getattr(a, k), getattr(b, k))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gated_block_graph(native, precision):
+    """A solver's first run launches its kernels one by one; later runs
+    replay the captured check block, a conditional graph whose body runs only
+    while the solve has not terminated.  The results are the first run's bit
+    for bit, and a replayed run launches fewer kernels than the first (the
+    block queued behind the one that ended the solve runs its gate alone)."""
+    from reformulation_b200 import pria
+    inst = jrp_demand(4, 40, 120)
+    launches, out = [], []
+    with pria.DeviceSolver(inst, pria.Library().parameters(-1, 1e-5), precision) as dev:
+        dev.set_megakernel(0)
+        for _ in range(3):
+            assert dev.run() == 0
+            out.append(dev.result(want_solution=True))
+            launches.append(dev.launches())
+    for b in out[1:]:
+        _same(out[0], b)
+    assert launches[1] < launches[0] and launches[2] == launches[1], launches
+
+
 @pytest.mark.parametrize("shape", [(10, 25), (30, 75), (4, 12), (7, 9)])
 def test_persistent_kernel_equals_graph_fp64(native, shape):
     from reformulation_b200 import pria
