@@ -368,6 +368,29 @@ def _same(a, b):
         assert np.array_equal(getattr(a, k), getattr(b, k))
 
 
+@pytest.mark.parametrize("precision,items", [("fp64", 20), ("f32", 40)])
+def test_large_solution_arrays_come_back_whole(lib, precision, items):
+    """Solution arrays of 16 MB and more come back through the library's
+    pinned ring, moved into the caller's arrays by several host threads: the
+    objective of the returned x, recomputed on the host, is the one the
+    device computed from its own copy, and x, y, z keep the solution's
+    structure (17.4 MB an array here, in either precision)."""
+    inst = jrp_demand(8, items, 330)
+    s = lib.solve(inst, lib.parameters(-1, 1e-4), precision, want_solution=True)
+    assert s.status == 0
+    assert s.x.nbytes >= 16 << 20
+    if precision == "fp64":
+        feasible(inst, s)
+    else:
+        upper = np.triu(np.ones((330, 330), bool))
+        assert np.all(s.x[:, ~upper] == 0) and np.all(s.y[:, ~upper] == 0)
+        assert np.allclose(s.x.sum(axis=1, dtype=np.float64), 1.0, atol=1e-4)
+    # the f32 solve holds H in FP32 (and takes it as FP32): its objective
+    # is the host's to FP32 rounding of H; FP64 to summation order
+    x = np.asarray(s.x, np.float64)
+    assert rel(lib.objective(inst, x), s.primal_objective) <= (1e-6 if precision == "f32" else 1e-12)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_gated_block_graph(native, precision):
     """A solver's first run launches its kernels one by one; later runs
