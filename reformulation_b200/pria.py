@@ -66,10 +66,10 @@ class Library:
 
     def solve(self, instance, parameters, precision: str = "fp64", want_solution: bool = False,
               warm=None) -> Solve:
-        k, k0, h = _arrays(instance)
         n, t = instance.items, instance.periods
         info = _native.PriaResultInfo()
         if precision == "fp64":
+            k, k0, h = _arrays(instance)
             out = [np.empty((n, t, t)) for _ in range(3)] if want_solution else [None] * 3
             w = [np.ascontiguousarray(a, np.float64) for a in warm] if warm else [None] * 3
             st = self._lib.pria_solve_f64(n, t, _native.dptr(k), k0, _native.dptr(h),
@@ -78,7 +78,11 @@ class Library:
                                           *[(_native.dptr(a) if a is not None else None) for a in out],
                                           ctypes.byref(info))
         else:
-            kf, hf = k.astype(np.float32), h.astype(np.float32)
+            # the f32 ABI takes float32 arrays: converted straight from the
+            # instance's own (no copy when it already holds float32)
+            kf = np.ascontiguousarray(instance.order_costs, np.float32)
+            hf = np.ascontiguousarray(instance.holding_costs, np.float32)
+            k0 = float(instance.joint_order_cost)
             out = [np.empty((n, t, t), np.float32) for _ in range(3)] if want_solution else [None] * 3
             w = [np.ascontiguousarray(a, np.float32) for a in warm] if warm else [None] * 3
             st = self._lib.pria_solve_f32(n, t, _native.fptr(kf), ctypes.c_float(k0),
