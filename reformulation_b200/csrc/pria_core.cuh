@@ -117,7 +117,7 @@ struct Params {
     double beta_sufficient, beta_necessary, beta_artificial;
     double theta_target, theta_decay;
     double scale;
-    long long start_max;     // step budget the start check judges against
+    long long start_max;     // step budget the start check compares against
     long long vanilla_max;   // step budget of the vanilla phase (< 0: none)
     double omega0;           // the initial primal weight
     int vanilla_solve;       // plain PDHG throughout (no Halpern phase)
